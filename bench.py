@@ -1,0 +1,374 @@
+#!/usr/bin/env python3
+"""Attempted Gay-Berne Monte Carlo moves per second on B200 (and the CPU reference).
+
+Workload (one system per GPU, weak scaling over GPUs): GB(kappa=3, kappa'=5,
+mu=2, nu=1), N = 1,048,576 ellipsoids, rho* = 0.32, T* = 0.8, cutoff 4.0,
+max displacement 0.1, max rotation 0.1, NVT, seeded simple-cubic lattice
+with orientations within 20 degrees of z; FP32 pair terms, FP64 state and
+sums.  A step is one checkerboard sweep (N trial moves).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  `value` times K sweeps with the state resident
+in HBM (CUDA events on the library's stream, max over ranks, L2 flushed
+between sweeps); `e2e` times the public C ABI with host arrays in pinned
+memory: upload + sweep + download every step.  `--impl reference` times the
+reference's own attempt_monte_carlo_move (MCnptColloid.c, built in
+oracle/_ref with its OpenMP pragmas) on the host cores.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "GB attempted moves/s"
+UNIT = "moves/s"
+N_PART = 1048576
+WORKLOAD = {
+    "workload": "Gay-Berne NVT sweep, N=1048576, rho*=0.32, T*=0.8, GB(3,5,2,1), rc=4.0, d=0.1, rot=0.1, "
+                "lattice start with orientations within 20 deg of z",
+    "n_particles": N_PART,
+    "precision": "fp32 pair terms, fp64 state and sums",
+}
+
+
+def gb_params(lcmc, seed):
+    return lcmc.default_params(
+        mc_ensemble_type=1, num_particles=N_PART, system_density=0.32, system_temperature=0.8,
+        gb_sigma_sidetoside=1.0, gb_epsilon0=1.0, gb_kappa=3.0, gb_kappa_prime=5.0, gb_mu_exponent=2.0,
+        gb_nu_exponent=1.0, max_displacement=0.1, max_rotation=0.1, cutoff_radius=4.0, verlet_radius=4.8,
+        colloid_wall_option=0, colloid_radius=0.0, init_orientation_cone_deg=20.0, precision_mode=1,
+        rng_seed=seed)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle/_ref/libmcref_omp.so: the reference's own functions)
+# ---------------------------------------------------------------------------
+def reference_cpu(n_part, seconds=12.0, threads=None):
+    """Time the reference's attempt_monte_carlo_move on the workload for about
+    `seconds` (a bounded sample).  The Verlet list (r_v = 4.8) is built once
+    with the same content as the reference's build_neighbor_lists (its O(N^2)
+    double loop is infeasible at N = 1M) and not rebuilt inside the sample,
+    which favours the reference."""
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import numpy as np
+
+    import oracle_ctypes as oc
+    so = os.path.join(REPO, "oracle", "_ref", "libmcref_omp.so")
+    if not os.path.exists(so):
+        return None, "oracle/_ref/libmcref_omp.so not built (needs the reference source at build time)"
+    threads = threads or os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    ref = C.CDLL(so)
+    D, DP, IP = C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_int)
+    ref.refdrv_set_box.argtypes = [C.c_int, DP]
+    ref.load_initial_conditions.argtypes = [C.c_char_p]
+    ref.refdrv_build_verlet_cells.argtypes = [DP, DP, DP, IP, IP, C.c_long]
+    ref.refdrv_build_verlet_cells.restype = C.c_long
+    ref.refdrv_run_attempts.argtypes = [C.c_long, C.c_int, DP, DP, DP, DP, DP, DP, IP, IP, C.c_long, DP,
+                                        C.POINTER(C.c_long), C.POINTER(C.c_long)]
+    ref.refdrv_run_attempts.restype = D
+    text = (f"mc_ensemble_type 1\nnum_particles {n_part}\nsystem_density 0.32\nsystem_temperature 0.8\n"
+            "system_pressure 2.0\ngb_sigma_sidetoside 1.0\ngb_epsilon0 1.0\ngb_kappa 3.0\ngb_kappa_prime 5.0\n"
+            "gb_mu_exponent 2.0\ngb_nu_exponent 1.0\nmax_displacement 0.1\nmax_rotation 0.1\n"
+            "initial_configuration_type 2\ncutoff_radius 4.0\nverlet_radius 4.8\ntotal_mc_cycles 1000\n"
+            "configuration_save_interval 100\nstatistics_print_interval 100\ncolloid_wall_option 0\n"
+            "colloid_interaction_epsilon 15\ncolloid_interaction_amplitude 1.5\ncolloid_radius 0.0\n")
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(text)
+        path = f.name
+    ref.load_initial_conditions(path.encode())
+    os.unlink(path)
+    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=n_part, rho=0.32, seed=1234, cone=20.0)
+    ref.refdrv_set_box(n_part, box.ctypes.data_as(DP))
+    libc = C.CDLL("libc.so.6")
+    libc.srand(1234)
+    ref.refdrv_fill_rotation_table()
+    arrs = [np.ascontiguousarray(a) for a in (px, py, pz, ox, oy, oz)]
+    ptrs = [a.ctypes.data_as(DP) for a in arrs]
+    cap = 200 * n_part
+    cnt = np.zeros(n_part, dtype=np.int32)
+    lst = np.zeros(cap, dtype=np.int32)
+    t0 = time.perf_counter()
+    if ref.refdrv_build_verlet_cells(*ptrs[:3], cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap) < 0:
+        return None, "Verlet list capacity"
+    t_list = time.perf_counter() - t0
+    E = D(0.0)
+    acc, nreb = C.c_long(0), C.c_long(0)
+    # calibrate, then a sample of about `seconds`
+    n_try = 20
+    dt = ref.refdrv_run_attempts(n_try, 0, *ptrs, cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap, C.byref(E),
+                                 C.byref(acc), C.byref(nreb))
+    n_att = max(50, int(n_try * seconds / max(dt, 1e-6)))
+    dt = ref.refdrv_run_attempts(n_att, 0, *ptrs, cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap, C.byref(E),
+                                 C.byref(acc), C.byref(nreb))
+    return {"value": n_att / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{n_att} attempt_monte_carlo_move calls (MCnptColloid.c:2445) at N={n_part} in {dt:.1f} s, "
+                      f"OpenMP threads={threads}, Verlet list (r_v=4.8) built once in {t_list:.1f} s and not rebuilt",
+            "seconds": dt}, None
+
+
+# ---------------------------------------------------------------------------
+# FP32 peak (for the roofline denominator): cuBLAS SGEMM, TF32 off
+# ---------------------------------------------------------------------------
+def fp32_peak_tflops(torch):
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def kernel_traffic():
+    """DRAM bytes per k_phase_fast launch from the committed ncu summary, or None."""
+    p = os.path.join(REPO, "profiles", "k_phase_fast_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        res, why = reference_cpu(N_PART, seconds=max(2.0, args.cpu_seconds))
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        steps = max(1, args.steps)
+        line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * N_PART / res["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded lattice)", "config": dict(WORKLOAD, parallelism="cpu openmp"),
+                "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import numpy as np
+    import torch
+
+    import parellel_mc_mpi_for_liquidcrystalsystems_b200 as lcmc
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    params = gb_params(lcmc, 1234 + rank)
+    s = lcmc.GBSystem(params)
+    s.get_initial_config()
+    ext = torch.cuda.ExternalStream(s.stream_handle())
+    for _ in range(max(3, args.warmup)):
+        s.sweep(1)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    st0 = s.stats()
+    step_ms, phase_ms = [], []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()  # evict the state from L2 between sweeps
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ext)
+            s.sweep(1)
+            b.record(ext)
+            b.synchronize()
+            step_ms.append(a.elapsed_time(b))
+            phase_ms.append(s.last_sweep_timing()[1])
+    torch.cuda.synchronize()
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    st1 = s.stats()
+    attempted = st1["attempted"] - st0["attempted"]
+    value = N_PART * args.steps * world / (total_ms * 1e-3)
+
+    # roofline of the colour-phase kernel: algorithmic flops per attempt
+    # 2 (8 C + 61 P): C = 27-cell stencil candidates, P = in-cutoff pairs per state
+    C_att = (st1["stencil_candidates"] - st0["stencil_candidates"]) / attempted
+    P2_att = (st1["pairs_in_cutoff"] - st0["pairs_in_cutoff"]) / attempted  # old + new states
+    flop_att = 16.0 * C_att + 61.0 * P2_att
+    launches_phase = 8
+    avg_launch_ms = statistics.mean(phase_ms) / launches_phase
+    flop_launch = flop_att * N_PART / launches_phase
+    achieved = flop_launch / (avg_launch_ms * 1e-3) / 1e12
+
+    # e2e through the C ABI: pinned host arrays, upload + sweep + download every step
+    state, box = s.download()
+    pinned = [torch.empty(N_PART, dtype=torch.float64, pin_memory=True) for _ in range(6)]
+    hv = [p.numpy() for p in pinned]
+    for h, x in zip(hv, state):
+        h[:] = x
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        s.upload(*hv, box)
+        s.sweep(1)
+        out, box = s.download()
+        for h, x in zip(hv, out):
+            h[:] = x
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = N_PART * args.e2e_steps * world / e2e_s
+    kps = s.kernels_per_sweep()
+    st = s.stats()
+    s.close()
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    peaks = measured_peaks()
+    sgemm = fp32_peak_tflops(torch)
+    nominal = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    cpu, why = reference_cpu(N_PART, seconds=args.cpu_seconds) if world == 1 else (None, "rank 0 of N>1")
+    clocks = clk.summary()
+    traffic = kernel_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded lattice, relaxing from the lattice start)",
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single system",
+                       l2="flushed between sweeps (256 MiB memset)"),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * N_PART + 4 * N_PART + 24,
+                "d2h_bytes_per_step": 6 * 8 * N_PART + 24},
+        "gpu_launches": kps * args.steps,
+        "roofline": {"bound": "fp32", "kernel": "k_phase_fast", "achieved": achieved, "peak": sgemm,
+                     "unit": "TFLOP/s", "frac": achieved / sgemm,
+                     "peak_source": "cuBLAS FP32 SGEMM (TF32 off) measured in this run; nominal FP32 "
+                                    f"{nominal:.1f} TFLOP/s at max clock",
+                     "traffic": traffic, "flop_per_attempt": flop_att, "stencil_candidates_per_attempt": C_att,
+                     "in_cutoff_pairs_per_attempt_old_plus_new": P2_att, "avg_launch_ms": avg_launch_ms,
+                     "phase_share_of_step": statistics.mean(phase_ms) / (total_ms / args.steps)},
+        "cpu_baseline": cpu if cpu else {"unavailable": why},
+        "acceptance": (st["accepted"] / max(st["attempted"], 1)),
+        "energy_per_particle": st["energy"] / N_PART,
+    }
+    if clocks:
+        line["clocks"] = clocks
+    if peaks:
+        line["measured_peaks"] = {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

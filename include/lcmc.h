@@ -1,0 +1,186 @@
+/*
+ * lcmc.h - C ABI of the B200 Gay-Berne Monte Carlo library (liblcmc.so).
+ *
+ * Drop-in for the Monte Carlo sweep of MCnptColloid.c.  The reference has no
+ * plugin or FFI layer; its seam is the C call
+ *
+ *   void attempt_monte_carlo_move(double *position_x, ..., double *orient_z,
+ *        float max_displacement, double *system_energy, int *neighbor_count_array,
+ *        int *neighbor_list_array, long *accepted_moves, double *desp_max,
+ *        size_t *histograma)                              (MCnptColloid.c:2445-2454)
+ *
+ * driven once per cycle by the serial loop at MCnptColloid.c:887-1032, with the
+ * intended per-cell loop of the MPI path at MCnptColloid.c:683-700.  This ABI
+ * replaces that loop: the caller's SoA double arrays are copied in, whole
+ * sweeps run on the GPU (8-colour checkerboard, one trial move per particle per
+ * sweep with the per-move semantics of attempt_monte_carlo_move), and the arrays
+ * are copied back.  Every function returns an int status: 0 = LCMC_OK, negative
+ * = LCMC_E* (the reference calls exit(1) instead).  There is no CPU fallback:
+ * without a CUDA device every device call returns LCMC_ENODEV.
+ *
+ * Threading: one host thread per context; a context owns one CUDA stream and
+ * is not reentrant.
+ */
+#ifndef LCMC_H
+#define LCMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LCMC_ABI_VERSION 1
+
+enum {
+    LCMC_OK = 0,
+    LCMC_EINVAL = -1,    /* bad argument */
+    LCMC_ENOFILE = -2,   /* parameter / configuration file cannot be opened */
+    LCMC_EPARAM = -3,    /* missing or unparsable parameter (load_initial_conditions exits here) */
+    LCMC_ECUDA = -4,     /* CUDA runtime error */
+    LCMC_ENOMEM = -5,    /* device or host allocation failed */
+    LCMC_ECELLCAP = -6,  /* a cell or its stencil holds more particles than the kernel's capacity */
+    LCMC_ENUMERIC = -7,  /* NaN or Inf energy */
+    LCMC_EBOX = -8,      /* box too small for the cutoff (L < 2 rc) or inconsistent sizes */
+    LCMC_ENODEV = -9,    /* no CUDA device */
+    LCMC_EOVERLAP = -10  /* a particle centre inside the colloid (check_no_colloid_overlaps, MCnptColloid.c:1324-1340) */
+};
+
+enum { LCMC_PREC_FP64 = 0, LCMC_PREC_FP32 = 1 };
+enum { LCMC_NVT = 1, LCMC_NPT = 2 };
+
+/* The 23 keys of parametersFile.txt (read by load_initial_conditions,
+ * MCnptColloid.c:3933-4133) and the keys this library adds.  Added keys are
+ * ignored with a warning by the reference parser (MCnptColloid.c:4093), so one
+ * file serves both. */
+typedef struct {
+    int mc_ensemble_type;            /* 1 = NVT, 2 = NPT */
+    int num_particles;
+    double system_density;
+    double system_temperature;
+    double system_pressure;
+    double gb_sigma_sidetoside;      /* sigma_0 */
+    double gb_epsilon0;
+    double gb_kappa;
+    double gb_kappa_prime;
+    double gb_mu_exponent;
+    double gb_nu_exponent;
+    float max_displacement;          /* full width of the trial translation */
+    float max_rotation;
+    int initial_configuration_type;  /* 0 file, 1 random, 2 lattice */
+    double cutoff_radius;
+    double verlet_radius;            /* parsed; the cell grid replaces the Verlet list */
+    int total_mc_cycles;
+    int configuration_save_interval;
+    int statistics_print_interval;
+    int colloid_wall_option;         /* 1 = colloid term on */
+    double colloid_interaction_epsilon;   /* parsed, unused (as in the reference) */
+    double colloid_interaction_amplitude; /* parsed, unused (as in the reference) */
+    double colloid_radius;
+    /* added keys */
+    uint64_t rng_seed;
+    int total_mc_sweeps;
+    int cell_capacity;               /* 0 = automatic */
+    double npt_max_dlnV;
+    int volume_moves_per_sweep;      /* 0 or 1 */
+    int precision_mode;              /* LCMC_PREC_FP64 / LCMC_PREC_FP32 */
+    double init_orientation_cone_deg;/* 180 = uniform on the sphere */
+    int n_read;                      /* out: number of reference keys found */
+    int missing_mask;                /* out: bit i = reference key i missing */
+} lcmc_params;
+
+typedef struct {
+    int64_t sweeps;              /* sweeps done on this replica */
+    int64_t attempted;           /* trial moves (one per particle per sweep) */
+    int64_t accepted;
+    int64_t hardcore_rejected;   /* trial centre inside the colloid */
+    int64_t volume_attempted;
+    int64_t volume_accepted;
+    double energy;               /* running total energy: last recompute + accepted dE (FP64) */
+    double box[3];
+    double last_recompute;       /* last FP64 total-energy recompute */
+    double drift;                /* running minus recomputed energy at the last recompute */
+    int64_t pairs_in_cutoff;     /* sum over attempts of in-cutoff pairs, old + new states */
+    int64_t stencil_candidates;  /* sum over attempts of 27-cell stencil candidates, excluding self */
+    int error_flags;             /* LCMC_F* bits seen by the kernels */
+    int kernel;                  /* 0 = FP64 kernel, 1 = FP32 kernel */
+} lcmc_stats;
+
+/* error_flags bits */
+enum {
+    LCMC_F_CELLCAP = 1,     /* cell above the active capacity: that cell made no moves */
+    LCMC_F_STENCILCAP = 2,  /* stencil above the candidate capacity: that cell made no moves */
+    LCMC_F_LISTCAP = 4,     /* neighbour-list capacity exceeded: that cell made no moves */
+    LCMC_F_NONFINITE = 8,   /* NaN/Inf energy change */
+    LCMC_F_GRIDCAP = 16     /* box grew past the allocated cell grid (cells kept wider) */
+};
+
+/* ---- parameters (host only) ---- */
+int lcmc_params_defaults(lcmc_params *p);
+/* load_initial_conditions (MCnptColloid.c:3933-4133): 23 required keys,
+ * unknown keys ignored, missing keys -> LCMC_EPARAM with p->missing_mask set. */
+int lcmc_params_load(const char *path, lcmc_params *p);
+
+/* ---- context ---- */
+typedef struct lcmc_ctx lcmc_ctx;
+/* One system (replica 0). */
+int lcmc_create(const lcmc_params *p, lcmc_ctx **out);
+/* n independent systems sweeping together in shared launches (replica r has params[r]). */
+int lcmc_create_batch(const lcmc_params *params, int n_replicas, lcmc_ctx **out);
+int lcmc_destroy(lcmc_ctx *ctx);
+int lcmc_num_replicas(const lcmc_ctx *ctx);
+
+/* get_initial_config (MCnptColloid.c:4215-4235) for initial_configuration_type 2:
+ * seeded simple-cubic lattice, box V = N/rho + V_colloid; uploads it. */
+int lcmc_init_config(lcmc_ctx *ctx, int replica);
+/* Host lattice only (no device): fills the caller's arrays and box. */
+int lcmc_lattice(const lcmc_params *p, int replica, double *px, double *py, double *pz, double *ox, double *oy,
+                 double *oz, double box[3]);
+
+/* Copy the caller's SoA arrays (positions in [0, L], orientations) to the
+ * device and recompute the total energy in FP64. */
+int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz, const double *ox,
+                const double *oy, const double *oz, int n, const double box[3]);
+int lcmc_download(lcmc_ctx *ctx, int replica, double *px, double *py, double *pz, double *ox, double *oy, double *oz,
+                  int n, double box[3]);
+
+/* n_sweeps checkerboard sweeps on every replica (each: N trial moves; NPT
+ * replicas add one ln V volume move per sweep). */
+int lcmc_sweep(lcmc_ctx *ctx, int n_sweeps);
+int lcmc_get_stats(lcmc_ctx *ctx, int replica, lcmc_stats *out);
+
+/* tot_ene (MCnptColloid.c:1598-1622): fresh total energy of one replica,
+ * pair terms in `precision`, sums in FP64.  Also resets the running energy. */
+int lcmc_total_energy(lcmc_ctx *ctx, int replica, int precision, double *energy);
+
+/* compute_liquid_crystal_order_parameters (MCnptColloid.c:2117-2218): Q tensor
+ * (xx, xy, xz, yy, yz, zz), P2 = 1.5 lambda_max and director. */
+int lcmc_order_parameter(lcmc_ctx *ctx, int replica, double Q[6], double *P2, double director[3]);
+
+/* Per-particle outcome of the last sweep, indexed by particle id:
+ * 0 rejected, 1 accepted, 2 colloid hard-core reject (for parity tests). */
+int lcmc_last_outcomes(lcmc_ctx *ctx, int replica, unsigned char *out, int n);
+
+/* Override the kernel choice (for tests): -1 auto, LCMC_PREC_FP64, LCMC_PREC_FP32. */
+int lcmc_set_kernel(lcmc_ctx *ctx, int kernel);
+
+/* ---- measurement (no counterpart in the reference, which only times with clock()) ---- */
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
+int lcmc_get_stream(lcmc_ctx *ctx, void **stream);
+/* Kernel launches in one sweep of this context (all replicas). */
+int lcmc_kernels_per_sweep(lcmc_ctx *ctx);
+/* Device time of the last sweep run by lcmc_sweep, part by part, from CUDA
+ * event nodes inside the sweep graph: ms[0] rebin, ms[1] the colour-phase
+ * kernels (all 8 phases), ms[2] volume move, ms[3] finalize. */
+int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4]);
+
+const char *lcmc_strerror(int code);
+/* Last error message of this context (or of the last failed create when ctx is NULL). */
+int lcmc_last_error(const lcmc_ctx *ctx, char *buf, size_t len);
+int lcmc_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

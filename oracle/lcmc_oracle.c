@@ -145,6 +145,8 @@ void lco_consts_from_params(const lco_params *p, int arith, lco_consts *c)
     c->coll_on = p->colloid_wall_option == 1;
     c->max_disp = (double)p->max_displacement;
     c->max_rot = (double)p->max_rotation;
+    c->wmin = p->cutoff_radius + (double)p->max_displacement;
+    if (p->mc_ensemble_type == 2) c->wmin *= 1.0 + p->npt_max_dlnV;
     c->arith = arith;
 }
 
@@ -625,12 +627,12 @@ int lco_init_lattice(const lco_params *p, int replica, double *px, double *py, d
 /* checkerboard cell grid                                                    */
 /* ------------------------------------------------------------------------ */
 
-/* Cells per axis: the largest even count whose width is >= rc + dmax (so that
- * same-colour cells never interact even after each particle has moved once by
- * up to dmax/2 per axis), or 1 when even 2 cells do not fit. */
-int lco_grid_dims(double L, double rc, double dmax, int *nc)
+/* Cells per axis: the largest even count whose width is >= wmin = rc + dmax
+ * (so that same-colour cells never interact even after each particle has moved
+ * once by up to dmax/2 per axis), or 1 when even 2 cells do not fit. */
+int lco_grid_dims(double L, double wmin, int *nc)
 {
-    int m = (int)floor(L / (rc + dmax));
+    int m = (int)floor(L / wmin);
     *nc = m >= 2 ? m - (m & 1) : 1;
     return 0;
 }
@@ -670,10 +672,10 @@ int lco_cell_of(double x, double shift, double w, int nc, double L)
 }
 
 int lco_grid_build(lco_grid *g, int n, const double *px, const double *py, const double *pz, const double box[3],
-                   double rc, double dmax, const double shift[3])
+                   double wmin, const double shift[3])
 {
     for (int k = 0; k < 3; k++) {
-        lco_grid_dims(box[k], rc, dmax, &g->nc[k]);
+        lco_grid_dims(box[k], wmin, &g->nc[k]);
         g->w[k] = box[k] / (double)g->nc[k];
         g->shift[k] = shift[k];
     }
@@ -757,11 +759,11 @@ int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n,
               int *order_out)
 {
     int nc[3];
-    for (int k = 0; k < 3; k++) lco_grid_dims(box[k], c->rc, c->max_disp, &nc[k]);
+    for (int k = 0; k < 3; k++) lco_grid_dims(box[k], c->wmin, &nc[k]);
     double shift[3];
     lco_sweep_shift(key, sweep, nc, box, shift);
     lco_grid g;
-    lco_grid_build(&g, n, px, py, pz, box, c->rc, c->max_disp, shift);
+    lco_grid_build(&g, n, px, py, pz, box, c->wmin, shift);
     int perm[8];
     lco_colour_order(key, sweep, perm);
     memset(st, 0, sizeof(*st));
@@ -857,7 +859,7 @@ double lco_total_energy_cells(const lco_consts *c, int n, const double *px, cons
 {
     lco_grid g;
     double zero[3] = {0, 0, 0};
-    lco_grid_build(&g, n, px, py, pz, box, c->rc, 0.0, zero);
+    lco_grid_build(&g, n, px, py, pz, box, c->rc, zero);
     double dumv = 0.0, wall = 0.0;
     for (int cz = 0; cz < g.nc[2]; cz++)
         for (int cy = 0; cy < g.nc[1]; cy++)

@@ -76,6 +76,8 @@ typedef struct {
     double coll_R, coll_cutoff;
     int coll_on;       /* colloid_wall_option == 1 */
     double max_disp, max_rot;
+    double wmin;       /* minimum checkerboard cell width: (rc + max_disp), times
+                          (1 + npt_max_dlnV) for NPT so scaled boxes keep rc */
     int arith;         /* LCO_ARITH_* */
 } lco_consts;
 
@@ -129,12 +131,12 @@ typedef struct {
     int *order;      /* particle ids, cell-major, ascending id inside a cell */
 } lco_grid;
 
-int lco_grid_dims(double L, double rc, double dmax, int *nc);
+int lco_grid_dims(double L, double wmin, int *nc);
 void lco_sweep_shift(const uint32_t key[2], uint64_t sweep, const int nc[3], const double box[3], double shift[3]);
 void lco_colour_order(const uint32_t key[2], uint64_t sweep, int perm[8]);
 int lco_cell_of(double x, double shift, double w, int nc, double L);
 int lco_grid_build(lco_grid *g, int n, const double *px, const double *py, const double *pz, const double box[3],
-                   double rc, double dmax, const double shift[3]);
+                   double wmin, const double shift[3]);
 void lco_grid_free(lco_grid *g);
 
 typedef struct {

@@ -1,0 +1,934 @@
+// lcmc_api.cu - host side of liblcmc.so: the C ABI declared in include/lcmc.h.
+//
+// Owns the device buffers of a batch of replicas, enqueues the per-sweep
+// kernels (rebin, 8 colour phases, optional volume move, finalize) on one
+// stream and replays them as CUDA graphs (one per buffer parity).
+#include <cuda_runtime.h>
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/lcmc.h"
+#include "lcmc_internal.h"
+#include "lcmc_launch.h"
+#include "lcmc_rng.cuh"
+
+using namespace lcmc;
+
+static thread_local std::string g_create_error;
+
+struct lcmc_ctx {
+    int R = 0;
+    int ntot = 0, ctot = 0;
+    std::vector<lcmc_params> params;
+    std::vector<Replica> rep; // host copy of the static part
+    cudaStream_t stream = nullptr;
+    int device = 0, sms = 148;
+    // device buffers
+    Replica *d_rep = nullptr;
+    DevStats *d_stats = nullptr;
+    int *d_act_off = nullptr, *d_p2r = nullptr;
+    double *d_x[2][6] = {{nullptr}};
+    int *d_id[2] = {nullptr, nullptr};
+    int *d_cid = nullptr, *d_rank = nullptr, *d_perm = nullptr, *d_scid = nullptr;
+    int *d_cell_count = nullptr, *d_cell_start = nullptr, *d_block_sums = nullptr;
+    double *d_cell_e0 = nullptr, *d_cell_e1 = nullptr;
+    int *d_cell_n0 = nullptr, *d_cell_n1 = nullptr;
+    unsigned long long *d_cell_pairs = nullptr, *d_cell_cands = nullptr;
+    unsigned char *d_outcome = nullptr;
+    double *d_pe0 = nullptr, *d_pe1 = nullptr;
+    int *d_phard = nullptr;
+    double *d_red = nullptr;
+    int cur = 0;
+    bool uploaded_all = false;
+    std::vector<char> uploaded;
+    // kernels
+    int kernel_override = -1;
+    int fast_variant = 0;
+    int grid_elem = 0, grid_exact = 0, grid_fast = 0;
+    bool any_fast = false, any_exact = false, any_npt = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool timed = false;
+    std::string err;
+};
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+static int set_err(lcmc_ctx *c, int code, const char *msg)
+{
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                                           \
+    do {                                                                                                              \
+        cudaError_t e_ = (call);                                                                                      \
+        if (e_ != cudaSuccess) {                                                                                      \
+            char b_[256];                                                                                             \
+            snprintf(b_, sizeof(b_), "%s: %s", #call, cudaGetErrorString(e_));                                        \
+            return set_err(ctx, e_ == cudaErrorMemoryAllocation ? LCMC_ENOMEM : LCMC_ECUDA, b_);                      \
+        }                                                                                                             \
+    } while (0)
+
+extern "C" const char *lcmc_strerror(int code)
+{
+    switch (code) {
+    case LCMC_OK: return "ok";
+    case LCMC_EINVAL: return "invalid argument";
+    case LCMC_ENOFILE: return "file cannot be opened";
+    case LCMC_EPARAM: return "missing or unparsable parameter";
+    case LCMC_ECUDA: return "CUDA error";
+    case LCMC_ENOMEM: return "out of memory";
+    case LCMC_ECELLCAP: return "cell or stencil above kernel capacity";
+    case LCMC_ENUMERIC: return "non-finite energy";
+    case LCMC_EBOX: return "box too small for the cutoff";
+    case LCMC_ENODEV: return "no CUDA device";
+    case LCMC_EOVERLAP: return "particle inside the colloid";
+    default: return "unknown error";
+    }
+}
+
+extern "C" int lcmc_last_error(const lcmc_ctx *ctx, char *buf, size_t len)
+{
+    if (!buf || len == 0) return LCMC_EINVAL;
+    const std::string &s = ctx ? ctx->err : g_create_error;
+    snprintf(buf, len, "%s", s.c_str());
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_abi_version(void) { return LCMC_ABI_VERSION; }
+
+// ---------------------------------------------------------------------------
+// parameters (load_initial_conditions, MCnptColloid.c:3933-4133)
+// ---------------------------------------------------------------------------
+
+static const char *kRefKeys[23] = {
+    "mc_ensemble_type", "num_particles", "system_density", "system_temperature", "system_pressure",
+    "gb_sigma_sidetoside", "gb_epsilon0", "gb_kappa", "gb_kappa_prime", "gb_mu_exponent", "gb_nu_exponent",
+    "max_displacement", "max_rotation", "initial_configuration_type", "cutoff_radius", "verlet_radius",
+    "total_mc_cycles", "configuration_save_interval", "statistics_print_interval", "colloid_wall_option",
+    "colloid_interaction_epsilon", "colloid_interaction_amplitude", "colloid_radius"};
+
+extern "C" int lcmc_params_defaults(lcmc_params *p)
+{
+    if (!p) return LCMC_EINVAL;
+    memset(p, 0, sizeof(*p));
+    p->mc_ensemble_type = LCMC_NVT;
+    p->num_particles = 1000;
+    p->system_density = 0.30;
+    p->system_temperature = 1.0;
+    p->system_pressure = 2.0;
+    p->gb_sigma_sidetoside = 1.0;
+    p->gb_epsilon0 = 1.0;
+    p->gb_kappa = 3.0;
+    p->gb_kappa_prime = 5.0;
+    p->gb_mu_exponent = 2.0;
+    p->gb_nu_exponent = 1.0;
+    p->max_displacement = 0.1f;
+    p->max_rotation = 0.1f;
+    p->initial_configuration_type = 2;
+    p->cutoff_radius = 4.0;
+    p->verlet_radius = 4.8;
+    p->total_mc_cycles = 1000;
+    p->configuration_save_interval = 100;
+    p->statistics_print_interval = 100;
+    p->colloid_wall_option = 0;
+    p->colloid_interaction_epsilon = 15.0;
+    p->colloid_interaction_amplitude = 1.5;
+    p->colloid_radius = 0.0;
+    p->rng_seed = 12345u;
+    p->total_mc_sweeps = 100;
+    p->cell_capacity = 0;
+    p->npt_max_dlnV = 0.01;
+    p->volume_moves_per_sweep = 1;
+    p->precision_mode = LCMC_PREC_FP32;
+    p->init_orientation_cone_deg = 180.0;
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_params_load(const char *path, lcmc_params *p)
+{
+    if (!path || !p) return LCMC_EINVAL;
+    FILE *f = fopen(path, "r");
+    if (!f) return set_err(nullptr, LCMC_ENOFILE, "cannot open parameter file");
+    char line[256], name[256], value[256];
+    int seen[23] = {0};
+    // read_next_parameter grammar (MCnptColloid.c:3894-3910)
+    while (fgets(line, sizeof(line), f)) {
+        if (line[0] == '\n' || line[0] == '#' || line[0] == '\0') continue;
+        value[0] = '\0';
+        if (sscanf(line, "%255s %255[^\n]", name, value) < 1) continue;
+        int k = -1;
+        for (int i = 0; i < 23; i++)
+            if (strcmp(name, kRefKeys[i]) == 0) k = i;
+        int ok = 1;
+        switch (k) {
+        case 0: ok = sscanf(value, "%d", &p->mc_ensemble_type); break;
+        case 1: ok = sscanf(value, "%d", &p->num_particles); break;
+        case 2: ok = sscanf(value, "%lf", &p->system_density); break;
+        case 3: ok = sscanf(value, "%lf", &p->system_temperature); break;
+        case 4: ok = sscanf(value, "%lf", &p->system_pressure); break;
+        case 5: ok = sscanf(value, "%lf", &p->gb_sigma_sidetoside); break;
+        case 6: ok = sscanf(value, "%lf", &p->gb_epsilon0); break;
+        case 7: ok = sscanf(value, "%lf", &p->gb_kappa); break;
+        case 8: ok = sscanf(value, "%lf", &p->gb_kappa_prime); break;
+        case 9: ok = sscanf(value, "%lf", &p->gb_mu_exponent); break;
+        case 10: ok = sscanf(value, "%lf", &p->gb_nu_exponent); break;
+        case 11: ok = sscanf(value, "%f", &p->max_displacement); break;
+        case 12: ok = sscanf(value, "%f", &p->max_rotation); break;
+        case 13: ok = sscanf(value, "%d", &p->initial_configuration_type); break;
+        case 14: ok = sscanf(value, "%lf", &p->cutoff_radius); break;
+        case 15: ok = sscanf(value, "%lf", &p->verlet_radius); break;
+        case 16: ok = sscanf(value, "%d", &p->total_mc_cycles); break;
+        case 17: ok = sscanf(value, "%d", &p->configuration_save_interval); break;
+        case 18: ok = sscanf(value, "%d", &p->statistics_print_interval); break;
+        case 19: ok = sscanf(value, "%d", &p->colloid_wall_option); break;
+        case 20: ok = sscanf(value, "%lf", &p->colloid_interaction_epsilon); break;
+        case 21: ok = sscanf(value, "%lf", &p->colloid_interaction_amplitude); break;
+        case 22: ok = sscanf(value, "%lf", &p->colloid_radius); break;
+        default:
+            if (strcmp(name, "rng_seed") == 0) {
+                unsigned long long s = 0;
+                ok = sscanf(value, "%llu", &s);
+                p->rng_seed = s;
+            } else if (strcmp(name, "total_mc_sweeps") == 0) ok = sscanf(value, "%d", &p->total_mc_sweeps);
+            else if (strcmp(name, "cell_capacity") == 0) ok = sscanf(value, "%d", &p->cell_capacity);
+            else if (strcmp(name, "npt_max_dlnV") == 0) ok = sscanf(value, "%lf", &p->npt_max_dlnV);
+            else if (strcmp(name, "volume_moves_per_sweep") == 0) ok = sscanf(value, "%d", &p->volume_moves_per_sweep);
+            else if (strcmp(name, "precision_mode") == 0) {
+                if (strncmp(value, "fp32", 4) == 0) p->precision_mode = LCMC_PREC_FP32;
+                else if (strncmp(value, "fp64", 4) == 0) p->precision_mode = LCMC_PREC_FP64;
+                else ok = sscanf(value, "%d", &p->precision_mode);
+            } else if (strcmp(name, "init_orientation_cone_deg") == 0)
+                ok = sscanf(value, "%lf", &p->init_orientation_cone_deg);
+            break; // other keys: ignored, as the reference only warns (MCnptColloid.c:4093)
+        }
+        if (ok != 1) {
+            fclose(f);
+            char b[300];
+            snprintf(b, sizeof(b), "cannot parse value of '%s'", name);
+            return set_err(nullptr, LCMC_EPARAM, b);
+        }
+        if (k >= 0) seen[k] = 1;
+    }
+    fclose(f);
+    p->n_read = 0;
+    p->missing_mask = 0;
+    for (int i = 0; i < 23; i++) {
+        if (seen[i]) p->n_read++;
+        else p->missing_mask |= 1 << i;
+    }
+    if (p->n_read != 23) return set_err(nullptr, LCMC_EPARAM, "not all 23 parameters were read");
+    return LCMC_OK;
+}
+
+// get_system_const (MCnptColloid.c:2752-2783) with chi after kappa^2.
+static void make_consts(const lcmc_params &p, GBConsts &k)
+{
+    memset(&k, 0, sizeof(k));
+    k.beta = 1.0 / p.system_temperature;
+    k.four_eps0 = 4.0 * p.gb_epsilon0;
+    k.rc = p.cutoff_radius;
+    k.rc2 = p.cutoff_radius * p.cutoff_radius;
+    k.sigma0 = p.gb_sigma_sidetoside;
+    double sigma_ee = p.gb_sigma_sidetoside * p.gb_kappa;
+    double k_imu = pow(p.gb_kappa_prime, 1.0 / p.gb_mu_exponent);
+    double kappa_sq = p.gb_kappa * p.gb_kappa;
+    k.chi = (kappa_sq - 1.0) / (kappa_sq + 1.0);
+    k.chi_sq = k.chi * k.chi;
+    k.chi_prime = (k_imu - 1.0) / (k_imu + 1.0);
+    k.mu = p.gb_mu_exponent;
+    k.nu = p.gb_nu_exponent;
+    k.kappa_prime = p.gb_kappa_prime;
+    k.coll_R = p.colloid_radius;
+    k.coll_cutoff = 4.0 * sigma_ee;
+    k.coll_on = p.colloid_wall_option == 1;
+    k.max_disp = (double)p.max_displacement;
+    k.max_rot = (double)p.max_rotation;
+    k.mu_code = p.gb_mu_exponent == 1.0 ? 1 : (p.gb_mu_exponent == 2.0 ? 2 : 0);
+    k.nu_code = p.gb_nu_exponent == 1.0 ? 1 : (p.gb_nu_exponent == 2.0 ? 2 : 0);
+    k.f_rc2 = (float)k.rc2;
+    k.f_chi = (float)k.chi;
+    k.f_chi_sq = (float)k.chi_sq;
+    k.f_chip = (float)k.chi_prime;
+    k.f_chip_sq = (float)(k.chi_prime * k.chi_prime);
+    k.f_sigma0 = (float)k.sigma0;
+    k.f_4eps0 = (float)k.four_eps0;
+    k.f_half_chi = (float)(0.5 * k.chi);
+    k.f_half_chip = (float)(0.5 * k.chi_prime);
+}
+
+static double min_cell_width(const lcmc_params &p)
+{
+    double w = p.cutoff_radius + (double)p.max_displacement;
+    if (p.mc_ensemble_type == LCMC_NPT) w *= 1.0 + p.npt_max_dlnV;
+    return w;
+}
+
+static int grid_dim_host(double L, double wmin)
+{
+    int m = (int)floor(L / wmin);
+    return m >= 2 ? m - (m & 1) : 1;
+}
+
+// ---------------------------------------------------------------------------
+// initial configuration (initialize_cubic_lattice_positions, MCnptColloid.c:2920-3033)
+// ---------------------------------------------------------------------------
+
+static double box_length(const lcmc_params &p)
+{
+    const double pi = 3.1415926535898; // MCnptColloid.c:10
+    double vcol = (4. / 3.) * pi * pow(p.colloid_radius, 3);
+    double V = (p.num_particles / p.system_density) + vcol; // MCnptColloid.c:2935
+    return pow(V, 1.0 / 3.0);
+}
+
+// Box V = N/rho + V_colloid; smallest n_s^3 lattice whose sites outside the
+// colloid hold N; spacing L/n_s without the reference's clamp to sigma_ee
+// (MCnptColloid.c:2957-2963 pushes sites outside the box when dense); sites
+// with |r - C|^2 <= R^2 skipped when R > 0; orientations uniform on the sphere
+// (Marsaglia, seeded) or uniform on the cap within init_orientation_cone_deg
+// of +z.
+extern "C" int lcmc_lattice(const lcmc_params *pp, int replica, double *px, double *py, double *pz, double *ox,
+                            double *oy, double *oz, double box[3])
+{
+    if (!pp || !px || !py || !pz || !ox || !oy || !oz || !box) return LCMC_EINVAL;
+    const lcmc_params &p = *pp;
+    const double pi = 3.1415926535898;
+    const int n = p.num_particles;
+    if (n <= 0 || p.system_density <= 0.0) return LCMC_EINVAL;
+    const double R = p.colloid_radius;
+    const double L = box_length(p);
+    box[0] = box[1] = box[2] = L;
+    const double C = 0.5 * L;
+    auto inside = [&](double x, double y, double z) {
+        double d[3] = {C - x, C - y, C - z};
+        for (int a = 0; a < 3; a++) {
+            if (d[a] > 0.5 * L) d[a] -= L;
+            else if (d[a] < -0.5 * L) d[a] += L;
+        }
+        double xs = d[0] * d[0], ys = d[1] * d[1], zs = d[2] * d[2];
+        double r2 = xs + ys + zs;
+        return R > 0.0 && r2 <= R * R;
+    };
+    int ns = 2;
+    for (;; ns++) {
+        long long free_sites = 0;
+        double d = L / (double)ns;
+        for (long long s = 0; s < (long long)ns * ns * ns; s++) {
+            double x = (double)(s % ns) * d, y = (double)((s / ns) % ns) * d, z = (double)(s / ((long long)ns * ns)) * d;
+            if (!inside(x, y, z)) free_sites++;
+        }
+        if (free_sites >= n) break;
+    }
+    const double delta = L / (double)ns;
+    uint32_t key[2];
+    (void)replica;
+    seed_key(p.rng_seed, key);
+    const double cone = p.init_orientation_cone_deg;
+    const double cmin = cos(cone * (pi / 180.0));
+    long long site = 0;
+    for (int i = 0; i < n; i++) {
+        double x, y, z;
+        for (;;) {
+            long long ix = site % ns, iy = (site / ns) % ns, iz = site / ((long long)ns * ns);
+            site++;
+            x = (double)ix * delta;
+            y = (double)iy * delta;
+            z = (double)iz * delta;
+            if (!inside(x, y, z)) break;
+        }
+        px[i] = x;
+        py[i] = y;
+        pz[i] = z;
+        if (cone >= 180.0) {
+            double v[3];
+            sphere_point(key, (uint32_t)i, INIT_SWEEP, v);
+            ox[i] = v[0];
+            oy[i] = v[1];
+            oz[i] = v[2];
+        } else {
+            U4 o = draw(key, (uint32_t)i, INIT_SWEEP, TAG_INIT);
+            double ct = 1.0 - u01(o.x) * (1.0 - cmin);
+            double st = sqrt(1.0 - ct * ct);
+            double ph = 2.0 * pi * u01(o.y);
+            ox[i] = st * cos(ph);
+            oy[i] = st * sin(ph);
+            oz[i] = ct;
+        }
+    }
+    return LCMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+static DevView view(const lcmc_ctx *c, int parity)
+{
+    DevView v;
+    memset(&v, 0, sizeof(v));
+    v.R = c->R;
+    v.ntot = c->ntot;
+    v.ctot = c->ctot;
+    v.rep = c->d_rep;
+    v.stats = c->d_stats;
+    v.act_off = c->d_act_off;
+    v.p2r = c->d_p2r;
+    const int a = parity, b = parity ^ 1;
+    v.px = c->d_x[a][0];
+    v.py = c->d_x[a][1];
+    v.pz = c->d_x[a][2];
+    v.ox = c->d_x[a][3];
+    v.oy = c->d_x[a][4];
+    v.oz = c->d_x[a][5];
+    v.id = c->d_id[a];
+    v.qx = c->d_x[b][0];
+    v.qy = c->d_x[b][1];
+    v.qz = c->d_x[b][2];
+    v.qux = c->d_x[b][3];
+    v.quy = c->d_x[b][4];
+    v.quz = c->d_x[b][5];
+    v.qid = c->d_id[b];
+    v.cid = c->d_cid;
+    v.scid = c->d_scid;
+    v.rank = c->d_rank;
+    v.perm = c->d_perm;
+    v.cell_count = c->d_cell_count;
+    v.cell_start = c->d_cell_start;
+    v.block_sums = c->d_block_sums;
+    v.cell_e0 = c->d_cell_e0;
+    v.cell_e1 = c->d_cell_e1;
+    v.cell_n0 = c->d_cell_n0;
+    v.cell_n1 = c->d_cell_n1;
+    v.cell_pairs = c->d_cell_pairs;
+    v.cell_cands = c->d_cell_cands;
+    v.outcome = c->d_outcome;
+    v.scratch_d = c->d_red;
+    return v;
+}
+
+static void free_ctx(lcmc_ctx *c)
+{
+    if (!c) return;
+    for (int i = 0; i < 2; i++)
+        if (c->graph[i]) cudaGraphExecDestroy(c->graph[i]);
+    for (int i = 0; i < 5; i++)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    void *ptrs[] = {c->d_rep, c->d_stats, c->d_act_off, c->d_p2r, c->d_id[0], c->d_id[1], c->d_cid, c->d_rank,
+                    c->d_perm, c->d_scid, c->d_cell_count, c->d_cell_start, c->d_block_sums, c->d_cell_e0,
+                    c->d_cell_e1, c->d_cell_n0, c->d_cell_n1, c->d_cell_pairs, c->d_cell_cands, c->d_outcome,
+                    c->d_pe0, c->d_pe1, c->d_phard, c->d_red};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (int a = 0; a < 2; a++)
+        for (int k = 0; k < 6; k++)
+            if (c->d_x[a][k]) cudaFree(c->d_x[a][k]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+template <typename T>
+static cudaError_t dalloc(T **p, size_t n)
+{
+    return cudaMalloc((void **)p, sizeof(T) * (n > 0 ? n : 1));
+}
+
+static void invalidate_graphs(lcmc_ctx *c)
+{
+    for (int i = 0; i < 2; i++)
+        if (c->graph[i]) {
+            cudaGraphExecDestroy(c->graph[i]);
+            c->graph[i] = nullptr;
+        }
+}
+
+// Kernel selection: FP32 kernel for precision_mode fp32 (boxes with >= 4
+// cells per axis; smaller boxes run the FP64 kernel), FP64 kernel otherwise.
+static void choose_kernels(lcmc_ctx *c)
+{
+    c->any_fast = c->any_exact = c->any_npt = false;
+    int need_amax = 0;
+    for (int r = 0; r < c->R; r++) {
+        Replica &rp = c->rep[r];
+        const lcmc_params &p = c->params[r];
+        int kern = c->kernel_override >= 0 ? c->kernel_override : (p.precision_mode == LCMC_PREC_FP32 ? 1 : 0);
+        rp.kernel = kern;
+        int nc = grid_dim_host(rp.L[0], rp.wmin);
+        if (kern == 1) {
+            c->any_fast = true;
+            if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
+            double wcell = rp.L[0] / (double)nc;
+            double mean = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]) * wcell * wcell * wcell;
+            int want = (int)(2.0 * mean + 16.0);
+            if (p.cell_capacity > want) want = p.cell_capacity;
+            if (want > need_amax) need_amax = want;
+        } else {
+            c->any_exact = true;
+        }
+        if (rp.ensemble == 2) c->any_npt = true;
+    }
+    c->fast_variant = need_amax > 48 ? 1 : 0;
+}
+
+static int upload_replica_table(lcmc_ctx *c)
+{
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_rep, c->rep.data(), sizeof(Replica) * c->R, cudaMemcpyHostToDevice, c->stream));
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **out)
+{
+    if (!params || n <= 0 || !out) return set_err(nullptr, LCMC_EINVAL, "bad arguments");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(nullptr, LCMC_ENODEV, "no CUDA device");
+    }
+    lcmc_ctx *c = new lcmc_ctx();
+    c->R = n;
+    c->params.assign(params, params + n);
+    c->rep.resize(n);
+    c->uploaded.assign(n, 0);
+    cudaGetDevice(&c->device);
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+    int poff = 0, coff = 0;
+    for (int r = 0; r < n; r++) {
+        const lcmc_params &p = params[r];
+        if (p.num_particles <= 0 || p.system_density <= 0.0 || p.system_temperature <= 0.0 || p.cutoff_radius <= 0.0) {
+            free_ctx(c);
+            return set_err(nullptr, LCMC_EINVAL, "bad parameters");
+        }
+        Replica &rp = c->rep[r];
+        memset(&rp, 0, sizeof(rp));
+        rp.n = p.num_particles;
+        rp.p_off = poff;
+        rp.ensemble = p.mc_ensemble_type == LCMC_NPT ? 2 : 1;
+        rp.pressure = p.system_pressure;
+        rp.dlnv_max = rp.ensemble == 2 && p.volume_moves_per_sweep > 0 ? p.npt_max_dlnV : 0.0;
+        rp.wmin = min_cell_width(p);
+        seed_key(p.rng_seed, rp.key);
+        make_consts(p, rp.k);
+        const double L = box_length(p);
+        rp.L[0] = rp.L[1] = rp.L[2] = L;
+        if (L < 2.0 * p.cutoff_radius) {
+            free_ctx(c);
+            return set_err(nullptr, LCMC_EBOX, "box shorter than twice the cutoff");
+        }
+        // cell grid capacity: NVT boxes keep their size; NPT boxes may grow (then cells stay wider)
+        double Lmax = rp.ensemble == 2 ? 1.25 * L : L;
+        rp.nc_max = grid_dim_host(Lmax, rp.wmin);
+        rp.cell_off = coff;
+        rp.sweep = 0ull;
+        poff += rp.n;
+        coff += rp.nc_max * rp.nc_max * rp.nc_max;
+    }
+    c->ntot = poff;
+    c->ctot = coff;
+#define ALLOC(ptr, cnt)                                                                                               \
+    do {                                                                                                              \
+        cudaError_t e_ = dalloc(&(ptr), (size_t)(cnt));                                                               \
+        if (e_ != cudaSuccess) {                                                                                      \
+            cudaGetLastError();                                                                                       \
+            free_ctx(c);                                                                                              \
+            return set_err(nullptr, LCMC_ENOMEM, "device allocation failed");                                         \
+        }                                                                                                             \
+    } while (0)
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        free_ctx(c);
+        return set_err(nullptr, LCMC_ECUDA, "stream creation failed");
+    }
+    for (int i = 0; i < 5; i++)
+        if (cudaEventCreate(&c->ev[i]) != cudaSuccess) {
+            free_ctx(c);
+            return set_err(nullptr, LCMC_ECUDA, "event creation failed");
+        }
+    ALLOC(c->d_rep, n);
+    ALLOC(c->d_stats, n);
+    ALLOC(c->d_act_off, 8 * (n + 1));
+    ALLOC(c->d_p2r, c->ntot);
+    for (int a = 0; a < 2; a++) {
+        for (int k = 0; k < 6; k++) ALLOC(c->d_x[a][k], c->ntot);
+        ALLOC(c->d_id[a], c->ntot);
+    }
+    ALLOC(c->d_cid, c->ntot);
+    ALLOC(c->d_rank, c->ntot);
+    ALLOC(c->d_perm, c->ntot);
+    ALLOC(c->d_scid, c->ntot);
+    ALLOC(c->d_cell_count, c->ctot);
+    ALLOC(c->d_cell_start, c->ctot + 1);
+    ALLOC(c->d_block_sums, 4096);
+    ALLOC(c->d_cell_e0, c->ctot);
+    ALLOC(c->d_cell_e1, c->ctot);
+    ALLOC(c->d_cell_n0, c->ctot);
+    ALLOC(c->d_cell_n1, c->ctot);
+    ALLOC(c->d_cell_pairs, c->ctot);
+    ALLOC(c->d_cell_cands, c->ctot);
+    ALLOC(c->d_outcome, c->ntot);
+    ALLOC(c->d_pe0, c->ntot);
+    ALLOC(c->d_pe1, c->ntot);
+    ALLOC(c->d_phard, c->ntot);
+    ALLOC(c->d_red, 16 * n + 16);
+#undef ALLOC
+    if ((c->ctot + 4095) / 4096 > 4096) {
+        free_ctx(c);
+        return set_err(nullptr, LCMC_EINVAL, "cell grid too large");
+    }
+    std::vector<int> p2r(c->ntot);
+    for (int r = 0; r < n; r++)
+        for (int i = 0; i < c->rep[r].n; i++) p2r[c->rep[r].p_off + i] = r;
+    cudaMemcpy(c->d_p2r, p2r.data(), sizeof(int) * c->ntot, cudaMemcpyHostToDevice);
+    cudaMemset(c->d_stats, 0, sizeof(DevStats) * n);
+    cudaMemset(c->d_outcome, 0, c->ntot);
+    cudaMemset(c->d_cell_e0, 0, sizeof(double) * c->ctot);
+    cudaMemset(c->d_cell_n0, 0, sizeof(int) * c->ctot);
+    cudaMemset(c->d_cell_n1, 0, sizeof(int) * c->ctot);
+    cudaMemset(c->d_cell_pairs, 0, sizeof(unsigned long long) * c->ctot);
+    cudaMemset(c->d_cell_cands, 0, sizeof(unsigned long long) * c->ctot);
+    choose_kernels(c);
+    c->grid_elem = 4 * c->sms;
+    c->grid_exact = 4 * c->sms;
+    c->grid_fast = fast_blocks_per_sm(c->fast_variant) * c->sms;
+    int rc = upload_replica_table(c);
+    if (rc) {
+        free_ctx(c);
+        return rc;
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        free_ctx(c);
+        return set_err(nullptr, LCMC_ECUDA, "initialisation failed");
+    }
+    *out = c;
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_create(const lcmc_params *p, lcmc_ctx **out) { return lcmc_create_batch(p, 1, out); }
+
+extern "C" int lcmc_destroy(lcmc_ctx *ctx)
+{
+    if (!ctx) return LCMC_EINVAL;
+    cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_num_replicas(const lcmc_ctx *ctx) { return ctx ? ctx->R : 0; }
+
+extern "C" int lcmc_set_kernel(lcmc_ctx *ctx, int kernel)
+{
+    if (!ctx || kernel < -1 || kernel > 1) return LCMC_EINVAL;
+    ctx->kernel_override = kernel;
+    // the device table keeps the dynamic fields; only `kernel` changes
+    for (int r = 0; r < ctx->R; r++) {
+        int kern = kernel >= 0 ? kernel : (ctx->params[r].precision_mode == LCMC_PREC_FP32 ? 1 : 0);
+        CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * r + offsetof(Replica, kernel), &kern,
+                                      sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    choose_kernels(ctx);
+    ctx->grid_fast = fast_blocks_per_sm(ctx->fast_variant) * ctx->sms;
+    invalidate_graphs(ctx);
+    return LCMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sweeps
+// ---------------------------------------------------------------------------
+
+// Rebin into the other buffer: afterwards the current buffer is cur ^ 1.
+static void enqueue_rebin(lcmc_ctx *c, int parity) { launch_rebin(view(c, parity), c->stream, c->grid_elem); }
+
+// One sweep; the event records become event nodes of the captured graph and
+// time its parts on the device (lcmc_last_sweep_timing).
+static void enqueue_sweep(lcmc_ctx *c, int parity)
+{
+    cudaEventRecord(c->ev[0], c->stream);
+    enqueue_rebin(c, parity);
+    cudaEventRecord(c->ev[1], c->stream);
+    DevView v = view(c, parity ^ 1);
+    for (int ci = 0; ci < 8; ci++) {
+        if (c->any_exact) launch_phase_exact(v, c->stream, ci, c->grid_exact);
+        if (c->any_fast) launch_phase_fast(c->fast_variant, v, c->stream, ci, c->grid_fast);
+    }
+    cudaEventRecord(c->ev[2], c->stream);
+    if (c->any_npt) launch_volume(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_exact);
+    cudaEventRecord(c->ev[3], c->stream);
+    launch_finalize(v, c->stream);
+    cudaEventRecord(c->ev[4], c->stream);
+}
+
+static int check_flags(lcmc_ctx *c)
+{
+    std::vector<DevStats> st(c->R);
+    CUDA_TRY(c, cudaMemcpyAsync(st.data(), c->d_stats, sizeof(DevStats) * c->R, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    int f = 0;
+    for (auto &s : st) f |= s.flags;
+    if (f & (F_CELLCAP | F_STENCILCAP | F_LISTCAP)) return set_err(c, LCMC_ECELLCAP, "cell capacity exceeded");
+    if (f & F_NONFINITE) return set_err(c, LCMC_ENUMERIC, "non-finite energy change");
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_sweep(lcmc_ctx *ctx, int n_sweeps)
+{
+    if (!ctx || n_sweeps < 0) return LCMC_EINVAL;
+    for (int r = 0; r < ctx->R; r++)
+        if (!ctx->uploaded[r]) return set_err(ctx, LCMC_EINVAL, "replica has no configuration (upload or init first)");
+    for (int s = 0; s < n_sweeps; s++) {
+        const int par = ctx->cur;
+        if (!ctx->graph[par]) {
+            cudaGraph_t g;
+            CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_sweep(ctx, par);
+            CUDA_TRY(ctx, cudaStreamEndCapture(ctx->stream, &g));
+            cudaError_t e = cudaGraphInstantiate(&ctx->graph[par], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                ctx->graph[par] = nullptr;
+                return set_err(ctx, LCMC_ECUDA, cudaGetErrorString(e));
+            }
+        }
+        CUDA_TRY(ctx, cudaGraphLaunch(ctx->graph[par], ctx->stream));
+        ctx->cur = par ^ 1;
+        ctx->timed = true;
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaGetLastError());
+    return check_flags(ctx);
+}
+
+extern "C" int lcmc_get_stream(lcmc_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream) return LCMC_EINVAL;
+    *stream = (void *)ctx->stream;
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
+{
+    if (!ctx) return LCMC_EINVAL;
+    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases; volume: propose, energy, accept, scale; finalize
+    return 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 4 * (int)ctx->any_npt + 1;
+}
+
+extern "C" int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4])
+{
+    if (!ctx || !ms) return LCMC_EINVAL;
+    if (!ctx->timed) return set_err(ctx, LCMC_EINVAL, "no sweep has run yet");
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < 4; i++) {
+        float t = 0.0f;
+        CUDA_TRY(ctx, cudaEventElapsedTime(&t, ctx->ev[i], ctx->ev[i + 1]));
+        ms[i] = t;
+    }
+    return LCMC_OK;
+}
+
+// Rebin (no sweep) and recompute the FP64 total energy of every replica with
+// the FP64 kernel; resets the running energies.
+static int recompute_energy(lcmc_ctx *c, int replica_only)
+{
+    enqueue_rebin(c, c->cur);
+    c->cur ^= 1;
+    DevView v = view(c, c->cur);
+    launch_energy_exact(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, 0, c->grid_exact);
+    launch_energy_reduce(v, c->stream, c->d_pe0, replica_only);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, cudaGetLastError());
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_total_energy(lcmc_ctx *ctx, int replica, int precision, double *energy)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !energy) return LCMC_EINVAL;
+    (void)precision; // pair terms of the recompute always run in FP64 (B200 FP64 rate is ample here)
+    int rc = recompute_energy(ctx, replica);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaMemcpy(energy, ctx->d_red + replica, sizeof(double), cudaMemcpyDeviceToHost));
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz,
+                           const double *ox, const double *oy, const double *oz, int n, const double box[3])
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !px || !py || !pz || !ox || !oy || !oz || !box)
+        return LCMC_EINVAL;
+    Replica &rp = ctx->rep[replica];
+    if (n != rp.n) return set_err(ctx, LCMC_EINVAL, "particle count differs from num_particles");
+    const double rc = ctx->params[replica].cutoff_radius;
+    for (int a = 0; a < 3; a++)
+        if (!(box[a] >= 2.0 * rc)) return set_err(ctx, LCMC_EBOX, "box shorter than twice the cutoff");
+    // check_no_colloid_overlaps (MCnptColloid.c:1324-1340) and the box bounds
+    const double R = ctx->params[replica].colloid_radius;
+    for (int i = 0; i < n; i++) {
+        if (!(px[i] >= 0.0 && px[i] <= box[0] && py[i] >= 0.0 && py[i] <= box[1] && pz[i] >= 0.0 && pz[i] <= box[2]))
+            return set_err(ctx, LCMC_EINVAL, "particle outside the box");
+        double dx = px[i] - 0.5 * box[0], dy = py[i] - 0.5 * box[1], dz = pz[i] - 0.5 * box[2];
+        if (dx * dx + dy * dy + dz * dz < R * R) return set_err(ctx, LCMC_EOVERLAP, "particle inside the colloid");
+        double n2 = ox[i] * ox[i] + oy[i] * oy[i] + oz[i] * oz[i];
+        if (!(n2 > 0.0) || !(n2 < 1e300)) return set_err(ctx, LCMC_EINVAL, "zero or non-finite orientation");
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const int off = rp.p_off;
+    const double *src[6] = {px, py, pz, ox, oy, oz};
+    for (int k = 0; k < 6; k++)
+        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_x[ctx->cur][k] + off, src[k], sizeof(double) * n, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+    std::vector<int> ids(n);
+    for (int i = 0; i < n; i++) ids[i] = i;
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_id[ctx->cur] + off, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    for (int a = 0; a < 3; a++) rp.L[a] = box[a];
+    // box (dynamic field) into the device table
+    CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * replica + offsetof(Replica, L), rp.L,
+                                  sizeof(double) * 3, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->uploaded[replica] = 1;
+    bool all = true;
+    for (int r = 0; r < ctx->R; r++) all = all && ctx->uploaded[r];
+    if (!all) return LCMC_OK; // energies are computed once every replica holds a configuration
+    int e = recompute_energy(ctx, -1);
+    if (e) return e;
+    // zero the drift of the first recompute
+    std::vector<DevStats> st(ctx->R);
+    CUDA_TRY(ctx, cudaMemcpy(st.data(), ctx->d_stats, sizeof(DevStats) * ctx->R, cudaMemcpyDeviceToHost));
+    for (auto &s : st) s.drift = 0.0;
+    CUDA_TRY(ctx, cudaMemcpy(ctx->d_stats, st.data(), sizeof(DevStats) * ctx->R, cudaMemcpyHostToDevice));
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_init_config(lcmc_ctx *ctx, int replica)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R) return LCMC_EINVAL;
+    const lcmc_params &p = ctx->params[replica];
+    const int n = p.num_particles;
+    std::vector<double> a(6 * (size_t)n);
+    double box[3];
+    int rc = lcmc_lattice(&p, replica, &a[0], &a[n], &a[2 * n], &a[3 * n], &a[4 * n], &a[5 * n], box);
+    if (rc) return rc;
+    return lcmc_upload(ctx, replica, &a[0], &a[n], &a[2 * n], &a[3 * n], &a[4 * n], &a[5 * n], n, box);
+}
+
+extern "C" int lcmc_download(lcmc_ctx *ctx, int replica, double *px, double *py, double *pz, double *ox, double *oy,
+                             double *oz, int n, double box[3])
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !px || !py || !pz || !ox || !oy || !oz) return LCMC_EINVAL;
+    const Replica &rp = ctx->rep[replica];
+    if (n != rp.n) return LCMC_EINVAL;
+    DevView v = view(ctx, ctx->cur);
+    launch_to_id_order(v, ctx->stream, replica, ctx->grid_elem);
+    double *dst[6] = {px, py, pz, ox, oy, oz};
+    const int other = ctx->cur ^ 1;
+    for (int k = 0; k < 6; k++)
+        CUDA_TRY(ctx, cudaMemcpyAsync(dst[k], ctx->d_x[other][k] + rp.p_off, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    if (box)
+        CUDA_TRY(ctx, cudaMemcpyAsync(box, (char *)ctx->d_rep + sizeof(Replica) * replica + offsetof(Replica, L),
+                                      sizeof(double) * 3, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_get_stats(lcmc_ctx *ctx, int replica, lcmc_stats *out)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !out) return LCMC_EINVAL;
+    DevStats s;
+    Replica rp;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&s, ctx->d_stats + replica, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(&rp, ctx->d_rep + replica, sizeof(rp), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    memset(out, 0, sizeof(*out));
+    out->sweeps = (int64_t)rp.sweep;
+    out->attempted = (int64_t)s.attempted;
+    out->accepted = (int64_t)s.accepted;
+    out->hardcore_rejected = (int64_t)s.hard;
+    out->volume_attempted = (int64_t)s.vol_att;
+    out->volume_accepted = (int64_t)s.vol_acc;
+    out->energy = s.energy;
+    out->box[0] = rp.L[0];
+    out->box[1] = rp.L[1];
+    out->box[2] = rp.L[2];
+    out->last_recompute = s.last_recompute;
+    out->drift = s.drift;
+    out->pairs_in_cutoff = (int64_t)s.pairs;
+    out->stencil_candidates = (int64_t)s.cands;
+    out->error_flags = s.flags;
+    out->kernel = rp.use_fast;
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_last_outcomes(lcmc_ctx *ctx, int replica, unsigned char *out, int n)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !out || n != ctx->rep[replica].n) return LCMC_EINVAL;
+    CUDA_TRY(ctx, cudaMemcpyAsync(out, ctx->d_outcome + ctx->rep[replica].p_off, (size_t)n, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return LCMC_OK;
+}
+
+// Q = <u u> - I/3, P2 = 1.5 lambda_max and its eigenvector (cyclic Jacobi,
+// Golub & Van Loan Alg. 8.4.3) - the reference's float Jacobi and its
+// largest-eigenvalue search (which starts at index 1, MCnptColloid.c:1890)
+// are replaced.
+extern "C" int lcmc_order_parameter(lcmc_ctx *ctx, int replica, double Q[6], double *P2, double director[3])
+{
+    if (!ctx || replica < 0 || replica >= ctx->R) return LCMC_EINVAL;
+    DevView v = view(ctx, ctx->cur);
+    launch_order_sums(v, ctx->stream, replica, ctx->d_red + 8 * ctx->R);
+    double s[6];
+    CUDA_TRY(ctx, cudaMemcpyAsync(s, ctx->d_red + 8 * ctx->R, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const double inv = 1.0 / (double)ctx->rep[replica].n;
+    double q[6] = {s[0] * inv - 1.0 / 3.0, s[1] * inv, s[2] * inv, s[3] * inv - 1.0 / 3.0, s[4] * inv,
+                   s[5] * inv - 1.0 / 3.0};
+    double a[3][3] = {{q[0], q[1], q[2]}, {q[1], q[3], q[4]}, {q[2], q[4], q[5]}};
+    double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int sweep = 0; sweep < 50; sweep++) {
+        double offd = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        if (offd < 1e-40) break;
+        for (int pp = 0; pp < 2; pp++)
+            for (int qq = pp + 1; qq < 3; qq++) {
+                if (a[pp][qq] == 0.0) continue;
+                double th = (a[qq][qq] - a[pp][pp]) / (2.0 * a[pp][qq]);
+                double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                double cs = 1.0 / sqrt(t * t + 1.0), sn = t * cs;
+                for (int k = 0; k < 3; k++) {
+                    double akp = a[k][pp], akq = a[k][qq];
+                    a[k][pp] = cs * akp - sn * akq;
+                    a[k][qq] = sn * akp + cs * akq;
+                }
+                for (int k = 0; k < 3; k++) {
+                    double apk = a[pp][k], aqk = a[qq][k];
+                    a[pp][k] = cs * apk - sn * aqk;
+                    a[qq][k] = sn * apk + cs * aqk;
+                }
+                for (int k = 0; k < 3; k++) {
+                    double vkp = V[k][pp], vkq = V[k][qq];
+                    V[k][pp] = cs * vkp - sn * vkq;
+                    V[k][qq] = sn * vkp + cs * vkq;
+                }
+            }
+    }
+    int im = 0;
+    for (int i = 1; i < 3; i++)
+        if (a[i][i] > a[im][im]) im = i;
+    if (Q)
+        for (int k = 0; k < 6; k++) Q[k] = q[k];
+    if (P2) *P2 = 1.5 * a[im][im];
+    if (director) {
+        director[0] = V[0][im];
+        director[1] = V[1][im];
+        director[2] = V[2][im];
+    }
+    return LCMC_OK;
+}

@@ -1,0 +1,32 @@
+// lcmc_launch.h - host-side launchers exported by the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lcmc_internal.h"
+
+namespace lcmc {
+
+// lcmc_rebin.cu
+void launch_rebin(const DevView &v, cudaStream_t s, int grid);
+void launch_finalize(const DevView &v, cudaStream_t s);
+
+// lcmc_sweep_exact.cu (FP64, bit-identical to the CPU oracle)
+void launch_phase_exact(const DevView &v, cudaStream_t s, int ci, int grid);
+void launch_energy_exact(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int scaled, int grid);
+
+// lcmc_sweep_fast.cu (FP32)
+struct FastVariant {
+    int threads, cpl, amax, lcap;
+};
+int fast_variant_count();
+FastVariant fast_variant(int i);
+void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, int grid);
+int fast_blocks_per_sm(int variant);
+
+// lcmc_misc.cu
+void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, int replica_only);
+void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid);
+void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out);
+void launch_to_id_order(const DevView &v, cudaStream_t s, int r, int grid);
+
+} // namespace lcmc

@@ -1,0 +1,305 @@
+// lcmc_rebin.cu - per-sweep grid set-up and the integer counting-sort rebin.
+//
+// The reference keeps a Verlet list rebuilt by an O(N^2) double loop
+// (build_neighbor_lists, MCnptColloid.c:1395-1468) and, in its MPI path,
+// scatters particles to 2x2x2 subcells of each rank's block
+// (dist_batch_to_cells, MCnptColloid.c:4942).  Here every sweep re-bins all
+// particles of all replicas into a cell grid (width >= rc + max_displacement)
+// with a randomly shifted origin:
+//   k_sweep_setup  grid size, shift and colour order per replica (Philox)
+//   k_bin          cell of every particle + arrival rank (atomics)
+//   k_scan_*       exclusive scan of the cell counts (3 kernels)
+//   k_scatter      slot of every particle
+//   k_sort_cells   inside every cell, ascending particle id (deterministic)
+//   k_gather       permute the SoA state into the other buffer
+// The result is bit-identical to the CPU oracle's grid (cell-major, id order).
+#include <cuda_runtime.h>
+
+#include "lcmc_internal.h"
+#include "lcmc_rng.cuh"
+
+namespace lcmc {
+
+__device__ __forceinline__ int grid_dim(double L, double wmin, int nc_max, int *flags)
+{
+    int m = (int)floor(L / wmin);
+    int nc = m >= 2 ? m - (m & 1) : 1;
+    if (nc > nc_max) {
+        nc = nc_max;
+        atomicOr(flags, F_GRIDCAP);
+    }
+    return nc;
+}
+
+// One block; thread r sets up replica r.  Then 8 threads scan the per-phase
+// active-cell counts over replicas.
+__global__ void k_sweep_setup(DevView v)
+{
+    for (int r = threadIdx.x; r < v.R; r += blockDim.x) {
+        Replica &p = v.rep[r];
+        for (int a = 0; a < 3; a++) {
+            p.nc[a] = grid_dim(p.L[a], p.wmin, p.nc_max, &v.stats[r].flags);
+            p.w[a] = p.L[a] / (double)p.nc[a];
+        }
+        U4 s = draw(p.key, SWEEP_ID, p.sweep, TAG_SHIFT);
+        p.shift[0] = u01(s.x) * p.w[0];
+        p.shift[1] = u01(s.y) * p.w[1];
+        p.shift[2] = u01(s.z) * p.w[2];
+        U4 c0 = draw(p.key, SWEEP_ID, p.sweep, TAG_COLOUR);
+        U4 c1 = draw(p.key, SWEEP_ID, p.sweep, TAG_COLOUR + 1);
+        uint32_t rr[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        int perm[8];
+        for (int i = 0; i < 8; i++) perm[i] = i;
+        for (int i = 7; i >= 1; i--) { // Fisher-Yates (the reference shuffles its subcells, 646-648)
+            int j = (int)(rr[7 - i] % (uint32_t)(i + 1));
+            int t = perm[i];
+            perm[i] = perm[j];
+            perm[j] = t;
+        }
+        for (int i = 0; i < 8; i++) p.perm[i] = perm[i];
+        p.use_fast = (p.kernel == 1) && p.nc[0] >= 4 && p.nc[1] >= 4 && p.nc[2] >= 4;
+        p.vol_state = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        int ci = threadIdx.x;
+        int *off = v.act_off + ci * (v.R + 1);
+        int acc = 0;
+        for (int r = 0; r < v.R; r++) {
+            off[r] = acc;
+            const Replica &p = v.rep[r];
+            int col = p.perm[ci];
+            int cnt = 1;
+            for (int a = 0; a < 3; a++) {
+                int b = (col >> a) & 1;
+                cnt *= (p.nc[a] - b + 1) / 2;
+            }
+            acc += cnt;
+        }
+        off[v.R] = acc;
+    }
+}
+
+__device__ __forceinline__ int cell_of(double x, double shift, double w, int nc, double L)
+{
+    double t = x - shift;
+    if (t < 0.0) t += L;
+    int c = (int)(t / w);
+    if (c >= nc) c = nc - 1;
+    if (c < 0) c = 0;
+    return c;
+}
+
+__global__ void k_bin(DevView v)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.ntot; i += gridDim.x * blockDim.x) {
+        const Replica &p = v.rep[v.p2r[i]];
+        int cx = cell_of(v.px[i], p.shift[0], p.w[0], p.nc[0], p.L[0]);
+        int cy = cell_of(v.py[i], p.shift[1], p.w[1], p.nc[1], p.L[1]);
+        int cz = cell_of(v.pz[i], p.shift[2], p.w[2], p.nc[2], p.L[2]);
+        int c = p.cell_off + (cz * p.nc[1] + cy) * p.nc[0] + cx;
+        v.cid[i] = c;
+        v.rank[i] = atomicAdd(&v.cell_count[c], 1);
+    }
+}
+
+// --- three-pass exclusive scan of cell_count -> cell_start (ctot + 1 entries) ---
+constexpr int SCAN_BLOCK = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+
+__device__ __forceinline__ int block_excl_scan(int x, int *sh, int *total)
+{
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) sh[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0;
+        int si = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += y;
+        }
+        sh[lane] = si - s;
+        if (lane == 31) sh[32] = si;
+    }
+    __syncthreads();
+    int r = inc - x + sh[w];
+    *total = sh[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_tiles(DevView v)
+{
+    __shared__ int sh[33];
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) s += (base + k < v.ctot) ? v.cell_count[base + k] : 0;
+    int tot;
+    block_excl_scan(s, sh, &tot);
+    if (threadIdx.x == 0) v.block_sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_sums(DevView v, int nblocks)
+{
+    __shared__ int sh[33];
+    // nblocks <= SCAN_BLOCK * SCAN_ITEMS (ctot <= 16.7 M cells)
+    int base = threadIdx.x * SCAN_ITEMS;
+    int loc[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        loc[k] = (base + k < nblocks) ? v.block_sums[base + k] : 0;
+        s += loc[k];
+    }
+    int tot;
+    int ex = block_excl_scan(s, sh, &tot);
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        if (base + k < nblocks) v.block_sums[base + k] = ex;
+        ex += loc[k];
+    }
+    if (threadIdx.x == 0) v.cell_start[v.ctot] = tot; // end sentinel = all particles
+}
+
+__global__ void k_scan_apply(DevView v)
+{
+    __shared__ int sh[33];
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int loc[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        loc[k] = (base + k < v.ctot) ? v.cell_count[base + k] : 0;
+        s += loc[k];
+    }
+    int tot;
+    int ex = block_excl_scan(s, sh, &tot) + v.block_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        if (base + k < v.ctot) v.cell_start[base + k] = ex;
+        ex += loc[k];
+    }
+}
+
+__global__ void k_scatter(DevView v)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.ntot; i += gridDim.x * blockDim.x)
+        v.perm[v.cell_start[v.cid[i]] + v.rank[i]] = i;
+}
+
+// Warp per cell: order the cell's slots by particle id (ids are unique inside
+// a replica).  Writes the gather source of every destination slot to `rank`
+// (reused as the second permutation buffer).
+__global__ void k_sort_cells(DevView v)
+{
+    int lane = threadIdx.x & 31;
+    int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < v.ctot; c += warps) {
+        int s = v.cell_start[c], e = v.cell_start[c + 1], n = e - s;
+        for (int a = lane; a < n; a += 32) {
+            int src = v.perm[s + a];
+            int my = v.id[src];
+            int rk = 0;
+            for (int b = 0; b < n; b++) rk += v.id[v.perm[s + b]] < my;
+            v.rank[s + rk] = src;
+        }
+    }
+}
+
+__global__ void k_gather(DevView v)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < v.ntot; g += gridDim.x * blockDim.x) {
+        int src = v.rank[g];
+        v.qx[g] = v.px[src];
+        v.qy[g] = v.py[src];
+        v.qz[g] = v.pz[src];
+        v.qux[g] = v.ox[src];
+        v.quy[g] = v.oy[src];
+        v.quz[g] = v.oz[src];
+        v.qid[g] = v.id[src];
+        v.scid[g] = v.cid[src];
+    }
+}
+
+// Block per replica: deterministic sums of the per-cell sweep results
+// (accepted dE, accepted count, hard-core rejects, pair/candidate counters).
+__global__ void k_sweep_finalize(DevView v)
+{
+    int r = blockIdx.x;
+    Replica &p = v.rep[r];
+    int c0 = p.cell_off, nc = p.nc[0] * p.nc[1] * p.nc[2];
+    double e = 0.0;
+    long long na = 0, nh = 0;
+    unsigned long long np = 0, ncand = 0;
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+        e += v.cell_e0[c0 + c];
+        na += v.cell_n0[c0 + c];
+        nh += v.cell_n1[c0 + c];
+        np += v.cell_pairs[c0 + c];
+        ncand += v.cell_cands[c0 + c];
+    }
+    __shared__ double se[256];
+    __shared__ long long sa[256], sh_[256];
+    __shared__ unsigned long long sp[256], sc[256];
+    se[threadIdx.x] = e;
+    sa[threadIdx.x] = na;
+    sh_[threadIdx.x] = nh;
+    sp[threadIdx.x] = np;
+    sc[threadIdx.x] = ncand;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            se[threadIdx.x] += se[threadIdx.x + o];
+            sa[threadIdx.x] += sa[threadIdx.x + o];
+            sh_[threadIdx.x] += sh_[threadIdx.x + o];
+            sp[threadIdx.x] += sp[threadIdx.x + o];
+            sc[threadIdx.x] += sc[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        DevStats &s = v.stats[r];
+        s.attempted += (unsigned long long)p.n;
+        s.accepted += (unsigned long long)sa[0];
+        s.hard += (unsigned long long)sh_[0];
+        s.pairs += sp[0];
+        s.cands += sc[0];
+        s.energy += se[0];
+        if (!(se[0] == se[0]) || se[0] - se[0] != 0.0) s.flags |= F_NONFINITE;
+        p.sweep += 1ull;
+    }
+}
+
+} // namespace lcmc
+
+#include "lcmc_launch.h"
+
+namespace lcmc {
+
+void launch_rebin(const DevView &v, cudaStream_t s, int grid)
+{
+    k_sweep_setup<<<1, 1024, 0, s>>>(v);
+    cudaMemsetAsync(v.cell_count, 0, sizeof(int) * (size_t)v.ctot, s);
+    k_bin<<<grid, 256, 0, s>>>(v);
+    const int tiles = (v.ctot + SCAN_TILE - 1) / SCAN_TILE;
+    k_scan_tiles<<<tiles, SCAN_BLOCK, 0, s>>>(v);
+    k_scan_sums<<<1, SCAN_BLOCK, 0, s>>>(v, tiles);
+    k_scan_apply<<<tiles, SCAN_BLOCK, 0, s>>>(v);
+    k_scatter<<<grid, 256, 0, s>>>(v);
+    k_sort_cells<<<grid, 256, 0, s>>>(v);
+    k_gather<<<grid, 256, 0, s>>>(v);
+}
+
+void launch_finalize(const DevView &v, cudaStream_t s) { k_sweep_finalize<<<v.R, 256, 0, s>>>(v); }
+
+} // namespace lcmc

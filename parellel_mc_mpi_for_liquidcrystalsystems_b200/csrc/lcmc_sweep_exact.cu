@@ -1,0 +1,318 @@
+// lcmc_sweep_exact.cu - FP64 checkerboard phase, bit-identical to the CPU oracle.
+//
+// Compiled with -fmad=false: every double operation is a single IEEE-rounded
+// +, -, *, / or sqrt, in the order of the reference's pij_GB / GBCollRod
+// (MCnptColloid.c:2607-2681, 1758-1854), so the accept/reject sequence equals
+// the oracle's canonical sweep.
+//
+// One warp per active cell.  The particles of the cell are attempted one after
+// another in ascending id (the reference picks a random particle per cycle,
+// MCnptColloid.c:2475; its MPI path loops over an active subcell's particles,
+// 683-700).  For each attempt the 32 lanes split the stencil slots q (q mod 32),
+// sum the old and new pair energies lane-locally in q order and combine them
+// with a xor butterfly: the canonical order the oracle reproduces.
+#include <cuda_runtime.h>
+
+#include "lcmc_gb.cuh"
+#include "lcmc_internal.h"
+#include "lcmc_rng.cuh"
+
+namespace lcmc {
+
+__device__ __forceinline__ int find_replica(const int *off, int R, int a)
+{
+    int lo = 0, hi = R;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= a) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double warp_sum_butterfly(double x)
+{
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) x = x + __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// apply_pbc (MCnptColloid.c:2420-2430)
+__device__ __forceinline__ void apply_pbc(double r[3], const double L[3])
+{
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (r[a] > L[a]) r[a] -= L[a];
+        else if (r[a] < 0.0) r[a] += L[a];
+    }
+}
+
+// Trial move of one particle (MCnptColloid.c:2502-2551 with Philox draws):
+// returns 0 if the colloid hard core rejects it (no energy evaluation).
+__device__ __forceinline__ int make_trial(const Replica &p, uint32_t id, const double ro[3], const double eo[3],
+                                          double rn[3], double en[3], double *u_acc)
+{
+    U4 m = draw(p.key, id, p.sweep, TAG_MOVE);
+    const double d = p.k.max_disp;
+    rn[0] = ro[0] + d * (u01(m.x) - 0.5);
+    rn[1] = ro[1] + d * (u01(m.y) - 0.5);
+    rn[2] = ro[2] + d * (u01(m.z) - 0.5);
+    *u_acc = u01(m.w);
+    apply_pbc(rn, p.L);
+    double c[3];
+    double r2 = dist_fold(rn[0], rn[1], rn[2], 0.5 * p.L[0], 0.5 * p.L[1], 0.5 * p.L[2], p.L, c);
+    if (!(r2 > p.k.coll_R * p.k.coll_R)) return 0;
+    double v[3];
+    sphere_point(p.key, id, p.sweep, v);
+    const double a = p.k.max_rot;
+    en[0] = a * v[0] + eo[0];
+    en[1] = a * v[1] + eo[1];
+    en[2] = a * v[2] + eo[2];
+    double n2 = en[0] * en[0] + en[1] * en[1] + en[2] * en[2];
+    if (n2 <= 1e-12) {
+        en[0] = eo[0];
+        en[1] = eo[1];
+        en[2] = eo[2];
+    } else {
+        double nr = __dsqrt_rn(n2);
+        en[0] /= nr;
+        en[1] /= nr;
+        en[2] /= nr;
+    }
+    return 1;
+}
+
+__global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
+{
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    __shared__ int s_cell[4][27];
+    __shared__ int s_base[4][28];
+    const int *off = v.act_off + ci * (v.R + 1);
+    const int total = off[v.R];
+    for (int a = blockIdx.x * nw + wib; a < total; a += gridDim.x * nw) {
+        const int r = find_replica(off, v.R, a);
+        const Replica &p = v.rep[r];
+        if (p.use_fast) continue;
+        const int col = p.perm[ci];
+        const int bx = col & 1, by = (col >> 1) & 1, bz = (col >> 2) & 1;
+        const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
+        const int nax = (nc0 - bx + 1) / 2, nay = (nc1 - by + 1) / 2;
+        int loc = a - off[r];
+        const int cx = 2 * (loc % nax) + bx;
+        loc /= nax;
+        const int cy = 2 * (loc % nay) + by;
+        const int cz = 2 * (loc / nay) + bz;
+        const int cell = p.cell_off + (cz * nc1 + cy) * nc0 + cx;
+
+        // canonical stencil: dz, dy, dx = -1..1, duplicates dropped at first occurrence
+        int c = -1;
+        if (lane < 27) {
+            int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dx = lane % 3 - 1;
+            int x = (cx + dx + nc0) % nc0, y = (cy + dy + nc1) % nc1, z = (cz + dz + nc2) % nc2;
+            c = p.cell_off + (z * nc1 + y) * nc0 + x;
+        }
+        unsigned same = __match_any_sync(0xffffffffu, c);
+        bool keep = lane < 27 && (__ffs(same) - 1) == lane;
+        unsigned kb = __ballot_sync(0xffffffffu, keep);
+        int ncell = __popc(kb);
+        int slot = __popc(kb & ((1u << lane) - 1u));
+        if (keep) s_cell[wib][slot] = c;
+        // exclusive prefix of counts over kept cells in slot order
+        int cnt_slot = 0;
+        __syncwarp();
+        if (lane < ncell) cnt_slot = v.cell_start[s_cell[wib][lane] + 1] - v.cell_start[s_cell[wib][lane]];
+        int inc = cnt_slot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane < ncell) s_base[wib][lane] = inc - cnt_slot;
+        if (lane == 31) s_base[wib][ncell] = inc;
+        __syncwarp();
+
+        const int cs = v.cell_start[cell], ce = v.cell_start[cell + 1];
+        double dE_sum = 0.0;
+        int nacc = 0, nhard = 0;
+        unsigned long long npairs = 0ull;
+        const unsigned long long cands = (unsigned long long)(s_base[wib][ncell] - 1) * (unsigned long long)(ce - cs);
+        for (int g = cs; g < ce; g++) {
+            const uint32_t id = (uint32_t)v.id[g];
+            double ro[3] = {v.px[g], v.py[g], v.pz[g]};
+            double eo[3] = {v.ox[g], v.oy[g], v.oz[g]};
+            double rn[3], en[3], uacc;
+            int ok = make_trial(p, id, ro, eo, rn, en, &uacc);
+            if (!ok) {
+                if (lane == 0) v.outcome[p.p_off + id] = 2;
+                nhard++;
+                continue;
+            }
+            double po = 0.0, pn = 0.0;
+            int np = 0;
+            for (int s = 0; s < ncell; s++) {
+                const int B = s_base[wib][s], n_s = s_base[wib][s + 1] - B;
+                const int g0 = v.cell_start[s_cell[wib][s]];
+                for (int q = B + ((lane - B) & 31); q < B + n_s; q += 32) {
+                    const int j = g0 + (q - B);
+                    if (j == g) continue;
+                    double rj[3] = {v.px[j], v.py[j], v.pz[j]};
+                    double ej[3] = {v.ox[j], v.oy[j], v.oz[j]};
+                    double d[3];
+                    double r2 = dist_fold(ro[0], ro[1], ro[2], rj[0], rj[1], rj[2], p.L, d);
+                    if (r2 < p.k.rc2) {
+                        po += pair_exact(p.k, r2, d, eo, ej);
+                        np++;
+                    }
+                    r2 = dist_fold(rn[0], rn[1], rn[2], rj[0], rj[1], rj[2], p.L, d);
+                    if (r2 < p.k.rc2) {
+                        pn += pair_exact(p.k, r2, d, en, ej);
+                        np++;
+                    }
+                }
+            }
+            double Eo = warp_sum_butterfly(po);
+            double En = warp_sum_butterfly(pn);
+            if (p.k.coll_on) {
+                Eo = Eo + colloid_rod(p.k, ro, eo, p.L);
+                En = En + colloid_rod(p.k, rn, en, p.L);
+            }
+            const double dE = En - Eo;
+            const bool acc = (dE <= 0.0) || (log_unit(uacc) <= -p.k.beta * dE);
+            npairs += (unsigned long long)np;
+            if (acc) {
+                if (lane == 0) {
+                    v.px[g] = rn[0];
+                    v.py[g] = rn[1];
+                    v.pz[g] = rn[2];
+                    v.ox[g] = en[0];
+                    v.oy[g] = en[1];
+                    v.oz[g] = en[2];
+                }
+                dE_sum += dE;
+                nacc++;
+            }
+            if (lane == 0) v.outcome[p.p_off + id] = acc ? 1 : 0;
+            __syncwarp();
+        }
+        // pair counter: sum over lanes
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
+        if (lane == 0) {
+            v.cell_e0[cell] = dE_sum;
+            v.cell_n0[cell] = nacc;
+            v.cell_n1[cell] = nhard;
+            v.cell_pairs[cell] = npairs;
+            v.cell_cands[cell] = cands;
+        }
+        __syncwarp();
+    }
+}
+
+// Warp per particle, FP64 exact arithmetic: E_i = sum over the 27-cell stencil
+// (j != i, r < rc, minimum image) in the canonical 32-way order; used for the
+// total energy (tot_ene, MCnptColloid.c:1598-1622) on any grid, including
+// boxes of fewer than 3 cells per axis.  With lam != 1 also the energy of the
+// configuration scaled by lam about the origin (NPT volume move), colloid at
+// the scaled box centre.  Outputs per particle slot: e0 (unscaled), e1 (scaled).
+__global__ void __launch_bounds__(128) k_energy_exact(DevView v, double *e0, double *e1, int *hard, int scaled)
+{
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    __shared__ int s_cell[4][27];
+    __shared__ int s_base[4][28];
+    for (int i = blockIdx.x * nw + wib; i < v.ntot; i += gridDim.x * nw) {
+        const int r = v.p2r[i];
+        const Replica &p = v.rep[r];
+        const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
+        if (scaled && p.ensemble != 2) continue;
+        const int cell = v.scid[i] - p.cell_off;
+        const int cx = cell % nc0, cy = (cell / nc0) % nc1, cz = cell / (nc0 * nc1);
+        int c = -1;
+        if (lane < 27) {
+            int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dx = lane % 3 - 1;
+            int x = (cx + dx + nc0) % nc0, y = (cy + dy + nc1) % nc1, z = (cz + dz + nc2) % nc2;
+            c = p.cell_off + (z * nc1 + y) * nc0 + x;
+        }
+        unsigned same = __match_any_sync(0xffffffffu, c);
+        bool keep = lane < 27 && (__ffs(same) - 1) == lane;
+        unsigned kb = __ballot_sync(0xffffffffu, keep);
+        int ncell = __popc(kb);
+        int slot = __popc(kb & ((1u << lane) - 1u));
+        if (keep) s_cell[wib][slot] = c;
+        __syncwarp();
+        int cnt_slot = 0;
+        if (lane < ncell) cnt_slot = v.cell_start[s_cell[wib][lane] + 1] - v.cell_start[s_cell[wib][lane]];
+        int inc = cnt_slot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane < ncell) s_base[wib][lane] = inc - cnt_slot;
+        if (lane == 31) s_base[wib][ncell] = inc;
+        __syncwarp();
+
+        const double lam = scaled ? p.vol_lambda : 1.0;
+        const double Ls[3] = {p.L[0] * lam, p.L[1] * lam, p.L[2] * lam};
+        double ri[3] = {v.px[i], v.py[i], v.pz[i]};
+        double ei[3] = {v.ox[i], v.oy[i], v.oz[i]};
+        double rs[3] = {ri[0] * lam, ri[1] * lam, ri[2] * lam};
+        double a0 = 0.0, a1 = 0.0;
+        for (int s = 0; s < ncell; s++) {
+            const int B = s_base[wib][s], n_s = s_base[wib][s + 1] - B;
+            const int g0 = v.cell_start[s_cell[wib][s]];
+            for (int q = B + ((lane - B) & 31); q < B + n_s; q += 32) {
+                const int j = g0 + (q - B);
+                if (j == i) continue;
+                double rj[3] = {v.px[j], v.py[j], v.pz[j]};
+                double ej[3] = {v.ox[j], v.oy[j], v.oz[j]};
+                double d[3];
+                double r2 = dist_fold(ri[0], ri[1], ri[2], rj[0], rj[1], rj[2], p.L, d);
+                if (r2 < p.k.rc2) a0 += pair_exact(p.k, r2, d, ei, ej);
+                if (scaled) {
+                    double rjs[3] = {rj[0] * lam, rj[1] * lam, rj[2] * lam};
+                    r2 = dist_fold(rs[0], rs[1], rs[2], rjs[0], rjs[1], rjs[2], Ls, d);
+                    if (r2 < p.k.rc2) a1 += pair_exact(p.k, r2, d, ei, ej);
+                }
+            }
+        }
+        a0 = warp_sum_butterfly(a0);
+        a1 = warp_sum_butterfly(a1);
+        if (lane == 0) {
+            double u0 = 0.5 * a0, u1 = 0.5 * a1;
+            if (p.k.coll_on) {
+                u0 += colloid_rod(p.k, ri, ei, p.L);
+                if (scaled) u1 += colloid_rod(p.k, rs, ei, Ls);
+            }
+            e0[i] = u0;
+            if (scaled) {
+                e1[i] = u1;
+                double d[3];
+                double r2 = dist_fold(rs[0], rs[1], rs[2], 0.5 * Ls[0], 0.5 * Ls[1], 0.5 * Ls[2], Ls, d);
+                hard[i] = !(r2 > p.k.coll_R * p.k.coll_R);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+} // namespace lcmc
+
+#include "lcmc_launch.h"
+
+namespace lcmc {
+
+void launch_phase_exact(const DevView &v, cudaStream_t s, int ci, int grid)
+{
+    k_phase_exact<<<grid, 128, 0, s>>>(v, ci);
+}
+
+void launch_energy_exact(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int scaled, int grid)
+{
+    k_energy_exact<<<grid, 128, 0, s>>>(v, e0, e1, hard, scaled);
+}
+
+} // namespace lcmc

@@ -1,0 +1,190 @@
+"""Python host mirror of the reference's Monte Carlo interface over liblcmc.so.
+
+Function names follow MCnptColloid.c (load_initial_conditions,
+get_initial_config, tot_ene, compute_liquid_crystal_order_parameters) so that
+driver code and tests read like the reference; every call goes through the C
+ABI of include/lcmc.h and runs on the GPU.  Errors raise LcmcError (the
+reference calls exit(1)).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import LcmcError, Params, Stats, check, lib
+
+
+def default_params(**overrides):
+    """lcmc_params with the library defaults, then `overrides` applied."""
+    p = Params()
+    check(lib().lcmc_params_defaults(C.byref(p)))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def load_initial_conditions(path, **overrides):
+    """Read a parametersFile.txt (MCnptColloid.c:3933-4133): the 23 keys of the
+    reference are required; added keys are optional."""
+    p = default_params()
+    rc = lib().lcmc_params_load(str(path).encode(), C.byref(p))
+    if rc != _lib.OK:
+        raise LcmcError(rc, f"{_lib.last_error()} (missing mask 0x{p.missing_mask:x})")
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def lattice(params, replica=0):
+    """Seeded simple-cubic start (initialize_cubic_lattice_positions,
+    MCnptColloid.c:2920-3033) computed on the host; returns (6 arrays, box)."""
+    n = params.num_particles
+    a = [np.zeros(n) for _ in range(6)]
+    box = np.zeros(3)
+    check(lib().lcmc_lattice(C.byref(params), replica, *[x.ctypes.data_as(_lib.DP) for x in a],
+                             box.ctypes.data_as(_lib.DP)))
+    return a, box
+
+
+def _dp(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_lib.DP)
+
+
+class GBSystem:
+    """One system or a batch of independent replicas on the GPU."""
+
+    def __init__(self, params):
+        if isinstance(params, Params):
+            params = [params]
+        arr = (Params * len(params))(*params)
+        h = C.c_void_p()
+        check(lib().lcmc_create_batch(arr, len(params), C.byref(h)))
+        self._h = h
+        self.params = list(params)
+        self.n_replicas = len(params)
+
+    # -- lifetime --
+    def close(self):
+        if self._h:
+            lib().lcmc_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        return check(rc, self._h)
+
+    # -- configuration --
+    def get_initial_config(self, replica=0):
+        """get_initial_config (MCnptColloid.c:4215-4235), lattice type: seeded
+        lattice uploaded to the device, FP64 total energy computed."""
+        self._check(lib().lcmc_init_config(self._h, replica))
+
+    def upload(self, px, py, pz, ox, oy, oz, box, replica=0):
+        arrs = [_dp(x) for x in (px, py, pz, ox, oy, oz)]
+        b, bp = _dp(box)
+        n = len(arrs[0][0])
+        self._check(lib().lcmc_upload(self._h, replica, *[p for _, p in arrs], n, bp))
+
+    def download(self, replica=0):
+        n = self.params[replica].num_particles
+        out = [np.zeros(n) for _ in range(6)]
+        box = np.zeros(3)
+        self._check(lib().lcmc_download(self._h, replica, *[x.ctypes.data_as(_lib.DP) for x in out], n,
+                                        box.ctypes.data_as(_lib.DP)))
+        return out, box
+
+    # -- Monte Carlo --
+    def sweep(self, n_sweeps=1):
+        """n_sweeps checkerboard sweeps (N attempts each) on every replica."""
+        self._check(lib().lcmc_sweep(self._h, n_sweeps))
+
+    def set_kernel(self, kernel):
+        """-1 automatic, 0 the FP64 kernel, 1 the FP32 kernel."""
+        self._check(lib().lcmc_set_kernel(self._h, kernel))
+
+    def stats(self, replica=0):
+        s = Stats()
+        self._check(lib().lcmc_get_stats(self._h, replica, C.byref(s)))
+        d = {k: getattr(s, k) for k, _ in Stats._fields_}
+        d["box"] = list(s.box)
+        return d
+
+    def tot_ene(self, replica=0):
+        """tot_ene (MCnptColloid.c:1598-1622): FP64 recompute of the total energy."""
+        e = C.c_double()
+        self._check(lib().lcmc_total_energy(self._h, replica, 0, C.byref(e)))
+        return e.value
+
+    def compute_liquid_crystal_order_parameters(self, replica=0):
+        """Q tensor (xx, xy, xz, yy, yz, zz), P2 and director (MCnptColloid.c:2117-2218)."""
+        Q = np.zeros(6)
+        P2 = C.c_double()
+        d = np.zeros(3)
+        self._check(lib().lcmc_order_parameter(self._h, replica, Q.ctypes.data_as(_lib.DP), C.byref(P2),
+                                               d.ctypes.data_as(_lib.DP)))
+        return Q, P2.value, d
+
+    # -- measurement --
+    def stream_handle(self):
+        """cudaStream_t of this context (as an integer) for event timing."""
+        s = C.c_void_p()
+        self._check(lib().lcmc_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def kernels_per_sweep(self):
+        return lib().lcmc_kernels_per_sweep(self._h)
+
+    def last_sweep_timing(self):
+        """Device ms of the last sweep by part: (rebin, colour phases, volume move, finalize)."""
+        ms = np.zeros(4)
+        self._check(lib().lcmc_last_sweep_timing(self._h, ms.ctypes.data_as(_lib.DP)))
+        return ms
+
+    def outcomes(self, replica=0):
+        """Per particle id, outcome of the last sweep: 0 reject, 1 accept, 2 hard-core reject."""
+        n = self.params[replica].num_particles
+        out = np.zeros(n, dtype=np.uint8)
+        self._check(lib().lcmc_last_outcomes(self._h, replica, out.ctypes.data_as(C.POINTER(C.c_ubyte)), n))
+        return out
+
+
+def run(params, n_sweeps, stats_interval=10, callback=None):
+    """Mirror of the reference's cycle loop (MCnptColloid.c:887-1061) at sweep
+    granularity: sweeps, running averages of E/N, rho and P2 every
+    `stats_interval` sweeps (update_running_averages, 2225-2260)."""
+    sums = {"E": 0.0, "rho": 0.0, "P2": 0.0, "n": 0}
+    with GBSystem(params) as s:
+        s.get_initial_config()
+        done = 0
+        while done < n_sweeps:
+            k = min(stats_interval, n_sweeps - done)
+            s.sweep(k)
+            done += k
+            st = s.stats()
+            _, P2, _ = s.compute_liquid_crystal_order_parameters()
+            V = st["box"][0] * st["box"][1] * st["box"][2]
+            rec = {"sweep": done, "E_per_N": st["energy"] / params.num_particles,
+                   "rho": params.num_particles / V, "P2": P2,
+                   "acceptance": st["accepted"] / max(st["attempted"], 1)}
+            sums["E"] += rec["E_per_N"]
+            sums["rho"] += rec["rho"]
+            sums["P2"] += rec["P2"]
+            sums["n"] += 1
+            if callback:
+                callback(rec)
+        n = max(sums["n"], 1)
+        return {"E_per_N": sums["E"] / n, "rho": sums["rho"] / n, "P2": sums["P2"] / n, "stats": s.stats()}

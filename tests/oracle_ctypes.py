@@ -42,7 +42,7 @@ class Consts(C.Structure):
     _fields_ = [(n, D) for n in ("beta", "four_eps0", "rc", "rc2", "sigma0", "sigma_ee", "kappa_sq", "chi",
                                  "chi_sq", "chi_prime", "k_imu", "mu", "nu", "kappa_prime", "coll_R",
                                  "coll_cutoff")] + [("coll_on", C.c_int), ("max_disp", D), ("max_rot", D),
-                                                     ("arith", C.c_int)]
+                                                     ("wmin", D), ("arith", C.c_int)]
 
 
 class SweepStats(C.Structure):
@@ -90,7 +90,7 @@ def lib():
         L.lco_key.argtypes = [C.c_uint64, C.c_int, U32P]
         L.lco_sphere_point.argtypes = [U32P, C.c_uint32, C.c_uint64, DP]
         L.lco_init_lattice.argtypes = [C.POINTER(Params), C.c_int, DP, DP, DP, DP, DP, DP, DP]
-        L.lco_grid_dims.argtypes = [D, D, D, IP]
+        L.lco_grid_dims.argtypes = [D, D, IP]
         L.lco_sweep_shift.argtypes = [U32P, C.c_uint64, IP, DP, DP]
         L.lco_colour_order.argtypes = [U32P, C.c_uint64, IP]
         L.lco_sweep.argtypes = [C.POINTER(Consts), U32P, C.c_uint64, C.c_int, DP, DP, DP, DP, DP, DP, DP,

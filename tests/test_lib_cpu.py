@@ -1,0 +1,109 @@
+"""CPU-side checks of the C ABI library (no GPU needed).
+
+* liblcmc.so loads and exports every function declared in include/lcmc.h;
+* the host-side parameter parser and lattice initialiser agree with the
+  oracle bit for bit;
+* without a GPU every device call fails loudly with LCMC_ENODEV (no CPU
+  fallback).
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle_ctypes as oc
+import parellel_mc_mpi_for_liquidcrystalsystems_b200 as lcmc
+from parellel_mc_mpi_for_liquidcrystalsystems_b200 import _lib
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def header_functions():
+    text = open(os.path.join(REPO, "include", "lcmc.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lcmc_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.lib()
+    names = header_functions()
+    assert len(names) >= 18
+    for name in names:
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (lcmc_\w+)", out))
+    assert set(names) <= exported
+    assert lib.lcmc_abi_version() == 1
+
+
+def test_params_parser_matches_oracle(golden):
+    text = bytes(golden("params_golden.npz")["text"]).decode()
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(text + "precision_mode fp64\nnpt_max_dlnV 0.02\nsomething_else 3\n")
+        path = f.name
+    try:
+        p = lcmc.load_initial_conditions(path)
+        q = oc.Params()
+        oc.lib().lco_params_defaults(C.byref(q))
+        assert oc.lib().lco_params_load(path.encode(), C.byref(q)) == 0
+    finally:
+        os.unlink(path)
+    for name, _ in oc.Params._fields_:
+        assert getattr(p, name) == getattr(q, name), name
+    assert p.precision_mode == 0 and p.npt_max_dlnV == 0.02
+
+
+def test_params_missing_key_raises(golden):
+    text = bytes(golden("params_golden.npz")["text"]).decode()
+    text = "\n".join(l for l in text.splitlines() if not l.startswith("cutoff_radius"))
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(text)
+        path = f.name
+    try:
+        with pytest.raises(lcmc.LcmcError) as e:
+            lcmc.load_initial_conditions(path)
+        assert e.value.code == _lib.EPARAM
+    finally:
+        os.unlink(path)
+    with pytest.raises(lcmc.LcmcError):
+        lcmc.load_initial_conditions("/nonexistent/parametersFile.txt")
+
+
+@pytest.mark.parametrize("n,rho,R,cone,seed", [
+    (1000, 0.30, 0.0, 180.0, 1), (4096, 0.32, 0.0, 20.0, 2), (3000, 0.30, 5.0, 180.0, 3), (777, 0.05, 2.0, 45.0, 4)])
+def test_lattice_matches_oracle_bitwise(n, rho, R, cone, seed):
+    p = lcmc.default_params(num_particles=n, system_density=rho, colloid_radius=R, init_orientation_cone_deg=cone,
+                            rng_seed=seed)
+    a, box = lcmc.lattice(p)
+    b = oc.init_lattice(n=n, rho=rho, R=R, cone=cone, seed=seed)
+    for x, y in zip(a, b[:6]):
+        assert np.array_equal(x, y)
+    assert np.array_equal(box, b[6])
+    # orientations are unit vectors, positions inside the box, none inside the colloid
+    assert np.allclose(a[3] ** 2 + a[4] ** 2 + a[5] ** 2, 1.0, atol=1e-14)
+    assert np.all((a[0] >= 0) & (a[0] < box[0]))
+    if R > 0:
+        d2 = sum((a[k] - box[k] / 2) ** 2 for k in range(3))
+        assert np.all(d2 > R * R)
+    if cone < 180:
+        assert np.all(a[5] >= np.cos(np.radians(cone)) - 1e-12)
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU error path")
+def test_no_gpu_is_a_loud_error():
+    p = lcmc.default_params(num_particles=1000)
+    with pytest.raises(lcmc.LcmcError) as e:
+        lcmc.GBSystem(p)
+    assert e.value.code == _lib.ENODEV
