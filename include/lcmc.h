@@ -175,6 +175,14 @@ int lcmc_kernels_per_sweep(lcmc_ctx *ctx);
  * kernels (all 8 phases), ms[2] volume move, ms[3] finalize. */
 int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4]);
 
+/* Gay-Berne pair term of n given configurations on the GPU, in the FP32
+ * kernel's arithmetic (out32) and in the FP64 kernel's arithmetic (out64):
+ * pij_GB (MCnptColloid.c:2618-2681) for separation d = r_j - r_i (3n values),
+ * orientations ei, ej (3n each), with the cutoff and the constants of p.
+ * Pairs beyond the cutoff give 0.  For tests and error statistics. */
+int lcmc_pair_terms(const lcmc_params *p, int n, const double *d, const double *ei, const double *ej, double *out32,
+                    double *out64);
+
 const char *lcmc_strerror(int code);
 /* Last error message of this context (or of the last failed create when ctx is NULL). */
 int lcmc_last_error(const lcmc_ctx *ctx, char *buf, size_t len);

@@ -28,6 +28,8 @@ SOURCES = {
     "lcmc_rebin.cu": [],
     "lcmc_misc.cu": ["-fmad=false"],
     "lcmc_api.cu": ["-fmad=false"],
+    "lcmc_pairtest.cu": [],
+    "lcmc_pairtest64.cu": ["-fmad=false"],
 }
 
 

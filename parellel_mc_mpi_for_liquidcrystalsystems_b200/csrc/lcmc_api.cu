@@ -707,6 +707,35 @@ extern "C" int lcmc_sweep(lcmc_ctx *ctx, int n_sweeps)
     return check_flags(ctx);
 }
 
+extern "C" int lcmc_pair_terms(const lcmc_params *p, int n, const double *d, const double *ei, const double *ej,
+                               double *out32, double *out64)
+{
+    if (!p || n < 0 || !d || !ei || !ej || !out32 || !out64) return LCMC_EINVAL;
+    if (n == 0) return LCMC_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(nullptr, LCMC_ENODEV, "no CUDA device");
+    }
+    GBConsts k;
+    make_consts(*p, k);
+    double *buf = nullptr;
+    const size_t b = sizeof(double) * (size_t)n;
+    if (cudaMalloc(&buf, 11 * b) != cudaSuccess) return set_err(nullptr, LCMC_ENOMEM, "device allocation failed");
+    double *dd = buf, *de = buf + 3 * (size_t)n, *dj = buf + 6 * (size_t)n, *o32 = buf + 9 * (size_t)n,
+           *o64 = buf + 10 * (size_t)n;
+    cudaMemcpy(dd, d, 3 * b, cudaMemcpyHostToDevice);
+    cudaMemcpy(de, ei, 3 * b, cudaMemcpyHostToDevice);
+    cudaMemcpy(dj, ej, 3 * b, cudaMemcpyHostToDevice);
+    launch_pair_terms32(k, n, dd, de, dj, o32, 0);
+    launch_pair_terms64(k, n, dd, de, dj, o64, 0);
+    cudaMemcpy(out32, o32, b, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(out64, o64, b, cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (e != cudaSuccess) return set_err(nullptr, LCMC_ECUDA, cudaGetErrorString(e));
+    return LCMC_OK;
+}
+
 extern "C" int lcmc_get_stream(lcmc_ctx *ctx, void **stream)
 {
     if (!ctx || !stream) return LCMC_EINVAL;

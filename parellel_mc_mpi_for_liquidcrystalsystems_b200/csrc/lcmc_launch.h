@@ -29,4 +29,10 @@ void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int
 void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out);
 void launch_to_id_order(const DevView &v, cudaStream_t s, int r, int grid);
 
+// lcmc_pairtest.cu / lcmc_pairtest64.cu (pair term on given inputs)
+void launch_pair_terms32(const GBConsts &k, int n, const double *d, const double *ei, const double *ej, double *out,
+                         cudaStream_t s);
+void launch_pair_terms64(const GBConsts &k, int n, const double *d, const double *ei, const double *ej, double *out,
+                         cudaStream_t s);
+
 } // namespace lcmc

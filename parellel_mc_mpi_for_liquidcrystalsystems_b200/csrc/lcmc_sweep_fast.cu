@@ -53,13 +53,25 @@ __device__ __forceinline__ int find_replica_f(const int *off, int R, int a)
 
 __device__ __forceinline__ int tri(int p, int q) { return (q * (q - 1)) / 2 + p; } // p < q
 
+// Coordinate relative to the active cell's origin o, folded by whole periods
+// into the window of the stencil cell it belongs to (centre cexp = (d + 1/2) w
+// for stencil offset d).  A stored coordinate may lie on either side of the
+// shifted periodic seam (cells that straddle it, or particles that crossed it
+// earlier in the sweep); the fold is exact because every particle stays within
+// w/2 + max_displacement/2 of its cell centre and w <= L/4.
+__device__ __forceinline__ double fold_rel(double x, double o, double cexp, double L)
+{
+    const double r = x - o;
+    return r - L * rint((r - cexp) / L);
+}
+
 template <int NT, int CPL, int AMAX, int LCAP>
 struct FastSmem {
     static constexpr int NW = NT / 32;
     static constexpr int SMAX = NT * CPL;
     static constexpr int NPAIR = AMAX * (AMAX - 1) / 2;
-    static_assert(3 * NPAIR <= 6 * SMAX, "in-cell pair arrays reuse the candidate region");
-    float cand[6 * SMAX]; // x | y | z | ux | uy | uz ; later tCA | tBA | cm
+    static constexpr int CAND = 6 * SMAX > 4 * NPAIR ? 6 * SMAX : 4 * NPAIR;
+    float cand[CAND]; // x | y | z | ux | uy | uz ; later the in-cell terms A | B | C | D
     float ax[AMAX], ay[AMAX], az[AMAX], aux[AMAX], auy[AMAX], auz[AMAX]; // old, relative
     float bx[AMAX], by[AMAX], bz[AMAX], bux[AMAX], buy[AMAX], buz[AMAX]; // new, relative
     float rad2[AMAX];
@@ -70,7 +82,6 @@ struct FastSmem {
     unsigned short list[NW][LCAP];
     unsigned short loff[NW][AMAX], lcnt[NW][AMAX];
     int st_start[27], st_cnt[27], st_pre[28];
-    int st_img[27];
     int wcnt[NW];
     int overflow;
     unsigned long long pairs;
@@ -82,7 +93,8 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
     using SM = FastSmem<NT, CPL, AMAX, LCAP>;
     constexpr int NW = SM::NW;
     constexpr int SMAX = SM::SMAX;
-    __shared__ SM sm;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SM &sm = *reinterpret_cast<SM *>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     float *cx_ = sm.cand, *cy_ = sm.cand + SMAX, *cz_ = sm.cand + 2 * SMAX;
     float *cux = sm.cand + 3 * SMAX, *cuy = sm.cand + 4 * SMAX, *cuz = sm.cand + 5 * SMAX;
@@ -135,7 +147,6 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
             int s = v.cell_start[c];
             sm.st_start[t] = s;
             sm.st_cnt[t] = v.cell_start[c + 1] - s;
-            sm.st_img[t] = (ix + 1) | ((iy + 1) << 2) | ((iz + 1) << 4);
         }
         if (t == 0) {
             sm.overflow = 0;
@@ -181,9 +192,12 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
             U4 m = draw(p.key, id, p.sweep, TAG_MOVE);
             double dsp[3] = {dmax * (u01(m.x) - 0.5), dmax * (u01(m.y) - 0.5), dmax * (u01(m.z) - 0.5)};
             double rn[3] = {ro[0] + dsp[0], ro[1] + dsp[1], ro[2] + dsp[2]};
-            // relative coordinates (unwrapped) for the pair terms
-            float xo = (float)(ro[0] - o0), yo = (float)(ro[1] - o1), zo = (float)(ro[2] - o2);
-            float xn = (float)(rn[0] - o0), yn = (float)(rn[1] - o1), zn = (float)(rn[2] - o2);
+            // coordinates relative to the cell origin (unwrapped) for the pair terms
+            const double qx = fold_rel(ro[0], o0, 0.5 * p.w[0], p.L[0]);
+            const double qy = fold_rel(ro[1], o1, 0.5 * p.w[1], p.L[1]);
+            const double qz = fold_rel(ro[2], o2, 0.5 * p.w[2], p.L[2]);
+            float xo = (float)qx, yo = (float)qy, zo = (float)qz;
+            float xn = (float)(qx + dsp[0]), yn = (float)(qy + dsp[1]), zn = (float)(qz + dsp[2]);
             for (int a3 = 0; a3 < 3; a3++) { // apply_pbc (MCnptColloid.c:2420-2430)
                 if (rn[a3] > p.L[a3]) rn[a3] -= p.L[a3];
                 else if (rn[a3] < 0.0) rn[a3] += p.L[a3];
@@ -257,13 +271,10 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
                     else hi = mid;
                 }
                 const int g = sm.st_start[s] + (f - sm.st_pre[s]);
-                const int img = sm.st_img[s];
-                const double sx = (double)((img & 3) - 1) * p.L[0];
-                const double sy = (double)(((img >> 2) & 3) - 1) * p.L[1];
-                const double sz = (double)(((img >> 4) & 3) - 1) * p.L[2];
-                x = (float)(v.px[g] + sx - o0);
-                y = (float)(v.py[g] + sy - o1);
-                z = (float)(v.pz[g] + sz - o2);
+                // stencil offset of slot s is (s % 3, s / 3 % 3, s / 9) - 1
+                x = (float)fold_rel(v.px[g], o0, ((double)(s % 3) - 0.5) * p.w[0], p.L[0]);
+                y = (float)fold_rel(v.py[g], o1, ((double)((s / 3) % 3) - 0.5) * p.w[1], p.L[1]);
+                z = (float)fold_rel(v.pz[g], o2, ((double)(s / 9) - 0.5) * p.w[2], p.L[2]);
                 float qx = fmaxf(fmaxf(-hb - x, x - (wx + hb)), 0.0f);
                 float qy = fmaxf(fmaxf(-hb - y, y - (wy + hb)), 0.0f);
                 float qz = fmaxf(fmaxf(-hb - z, z - (wz + hb)), 0.0f);
@@ -371,7 +382,9 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
 #pragma unroll
             for (int i = 0; i < NW; i++) pre[i + 1] = pre[i] + sm.lcnt[i][k];
             const int T = pre[NW];
-            float so = 0.0f, sn = 0.0f;
+            // FP64 lane sums: the 1e9 overlap clamp is exact in FP32 and must
+            // cancel exactly between the old and the new sum
+            double so = 0.0, sn = 0.0;
             int np = 0;
             for (int q = lane; q < T; q += 32) {
                 int ww = 0;
@@ -384,7 +397,7 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
                 float r2 = dx * dx + dy * dy + dz * dz;
                 float e = pair_fast(K, dx, dy, dz, r2, uox, uoy, uoz, ujx, ujy, ujz);
                 bool in = r2 < K.rc2;
-                so += in ? e : 0.0f;
+                so += in ? (double)e : 0.0;
                 np += in;
                 dx = xj - xn;
                 dy = yj - yn;
@@ -392,10 +405,10 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
                 r2 = dx * dx + dy * dy + dz * dz;
                 e = pair_fast(K, dx, dy, dz, r2, unx, uny, unz, ujx, ujy, ujz);
                 in = r2 < K.rc2;
-                sn += in ? e : 0.0f;
+                sn += in ? (double)e : 0.0;
                 np += in;
             }
-            double dso = (double)so, dsn = (double)sn;
+            double dso = so, dsn = sn;
 #pragma unroll
             for (int o = 16; o >= 1; o >>= 1) {
                 dso += __shfl_xor_sync(0xffffffffu, dso, o);
@@ -411,7 +424,7 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
         __syncthreads();
 
         // ---- 6 in-cell pairs: 4 terms per unordered pair (reuses the candidate region) ----
-        float *tCA = sm.cand, *tBA = sm.cand + SM::NPAIR, *tcm = sm.cand + 2 * SM::NPAIR;
+        float *tA = sm.cand, *tB = sm.cand + SM::NPAIR, *tC = sm.cand + 2 * SM::NPAIR, *tD = sm.cand + 3 * SM::NPAIR;
         const int npair = na * (na - 1) / 2;
         int npin = 0;
         for (int idx = t; idx < npair; idx += NT) {
@@ -451,21 +464,28 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
                                            sm.buy[q], sm.buz[q])
                                : 0.0f;
             }
-            tCA[idx] = C - A;
-            tBA[idx] = B - A;
-            tcm[idx] = (D - C) - (B - A);
+            // the four terms as computed (the 1e9 clamp is exact); differences are taken in FP64
+            tA[idx] = A;
+            tB[idx] = B;
+            tC[idx] = C;
+            tD[idx] = D;
         }
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) npin += __shfl_xor_sync(0xffffffffu, npin, o);
         if (lane == 0 && npin) atomicAdd(&sm.pairs, (unsigned long long)npin);
         __syncthreads();
         for (int k = t; k < na; k += NT) {
-            float dsum = 0.0f;
+            double dsum = 0.0;
             for (int m = 0; m < na; m++) {
-                if (m < k) dsum += tBA[tri(m, k)];
-                else if (m > k) dsum += tCA[tri(k, m)];
+                if (m < k) {
+                    const int i2 = tri(m, k); // k is the later particle: phi(n_k, o_m) - phi(o_k, o_m)
+                    dsum += (double)tB[i2] - (double)tA[i2];
+                } else if (m > k) {
+                    const int i2 = tri(k, m); // k is the earlier particle
+                    dsum += (double)tC[i2] - (double)tA[i2];
+                }
             }
-            sm.dEk[k] = (sm.Snew[k] - sm.Sold[k]) + (double)dsum + sm.dUc[k];
+            sm.dEk[k] = (sm.Snew[k] - sm.Sold[k]) + dsum + sm.dUc[k];
         }
         __syncthreads();
 
@@ -485,8 +505,15 @@ __global__ void __launch_bounds__(NT) k_phase_fast(DevView v, int ci)
                 if (acc) {
                     dsum += val;
                     nacc++;
-                    if (lane > m && lane < na) e0 += (double)tcm[tri(m, lane)];
-                    if (lane + 32 > m && lane + 32 < na) e1 += (double)tcm[tri(m, lane + 32)];
+                    // c(k, m) = [phi(n_k, n_m) - phi(o_k, n_m)] - [phi(n_k, o_m) - phi(o_k, o_m)]
+                    if (lane > m && lane < na) {
+                        const int i2 = tri(m, lane);
+                        e0 += ((double)tD[i2] - (double)tC[i2]) - ((double)tB[i2] - (double)tA[i2]);
+                    }
+                    if (lane + 32 > m && lane + 32 < na) {
+                        const int i2 = tri(m, lane + 32);
+                        e1 += ((double)tD[i2] - (double)tC[i2]) - ((double)tB[i2] - (double)tA[i2]);
+                    }
                 }
                 if (lane == 0) sm.acc[m] = acc;
             }
@@ -535,24 +562,41 @@ static const FastVariant kVariants[] = {{128, 6, 48, 1024}, {128, 8, 64, 1536}, 
 int fast_variant_count() { return (int)(sizeof(kVariants) / sizeof(kVariants[0])); }
 FastVariant fast_variant(int i) { return kVariants[i]; }
 
+template <int NT, int CPL, int AMAX, int LCAP>
+static void launch_v(const DevView &v, cudaStream_t s, int ci, int grid)
+{
+    const int bytes = (int)sizeof(FastSmem<NT, CPL, AMAX, LCAP>);
+    k_phase_fast<NT, CPL, AMAX, LCAP><<<grid, NT, bytes, s>>>(v, ci);
+}
+
+template <int NT, int CPL, int AMAX, int LCAP>
+static int occupancy_v()
+{
+    const int bytes = (int)sizeof(FastSmem<NT, CPL, AMAX, LCAP>);
+    cudaFuncSetAttribute(k_phase_fast<NT, CPL, AMAX, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_phase_fast<NT, CPL, AMAX, LCAP>, NT, bytes);
+    return n > 0 ? n : 1;
+}
+
 void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, int grid)
 {
     switch (variant) {
-    case 0: k_phase_fast<128, 6, 48, 1024><<<grid, 128, 0, s>>>(v, ci); break;
-    case 1: k_phase_fast<128, 8, 64, 1536><<<grid, 128, 0, s>>>(v, ci); break;
-    default: k_phase_fast<256, 4, 64, 768><<<grid, 256, 0, s>>>(v, ci); break;
+    case 0: launch_v<128, 6, 48, 1024>(v, s, ci, grid); break;
+    case 1: launch_v<128, 8, 64, 1536>(v, s, ci, grid); break;
+    default: launch_v<256, 4, 64, 768>(v, s, ci, grid); break;
     }
 }
 
+// Also opts the variant in to its dynamic shared memory size: call once
+// before the first launch of a variant.
 int fast_blocks_per_sm(int variant)
 {
-    int n = 0;
     switch (variant) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_phase_fast<128, 6, 48, 1024>, 128, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_phase_fast<128, 8, 64, 1536>, 128, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_phase_fast<256, 4, 64, 768>, 256, 0); break;
+    case 0: return occupancy_v<128, 6, 48, 1024>();
+    case 1: return occupancy_v<128, 8, 64, 1536>();
+    default: return occupancy_v<256, 4, 64, 768>();
     }
-    return n > 0 ? n : 1;
 }
 
 } // namespace lcmc

@@ -160,13 +160,15 @@ def test_fp32_kernel_agrees_with_fp64():
     decisions except where dE is within FP32 rounding of the Metropolis
     threshold; the FP32 running energy (FP32 pair terms, FP64 sums) stays
     within 2e-6 relative of the FP64 recompute."""
-    lp, _ = params_pair(11000, 0.30, 41, precision_mode=0)
+    lp, _ = params_pair(11000, 0.08, 41, precision_mode=0)
     state, box = start_state(lp)
     with lcmc.GBSystem(lp) as s:
         s.set_kernel(0)
         s.upload(*state, box)
-        s.sweep(30)  # relax the overlapped lattice with the FP64 kernel
+        s.sweep(100)  # relax the lattice with the FP64 kernel
         relaxed, rbox = s.download()
+        e_relaxed = s.tot_ene() / 11000
+    assert e_relaxed < 0.0  # no overlapping pairs left
     res = {}
     for kern in (0, 1):
         with lcmc.GBSystem(lp) as s:
@@ -179,10 +181,54 @@ def test_fp32_kernel_agrees_with_fp64():
                 assert st["kernel"] == 1
     o64, o32 = res[0][0], res[1][0]
     agree = np.mean(o64 == o32)
+    print(f"relaxed E/N {e_relaxed:.4g}; outcome agreement {agree:.5f}; "
+          f"acceptance fp64 {np.mean(o64 == 1):.4f} fp32 {np.mean(o32 == 1):.4f}")
     assert agree >= 0.995, agree
     st32, e32 = res[1][1], res[1][2]
     assert abs(st32["energy"] - e32) <= 2e-6 * abs(e32) + 1e-3
     assert st32["pairs_in_cutoff"] > 0 and st32["stencil_candidates"] > st32["pairs_in_cutoff"] // 2
+
+
+def test_pair_terms_fp64_bitwise_and_fp32_error():
+    """Pair term on the GPU: the FP64 kernel's arithmetic equals the oracle's
+    canonical pij_GB bit for bit.  FP32 error relative to max(|phi|, 1),
+    measured on B200 over 1.8e5 random in-cutoff pairs: median 1.8e-8, p99
+    2.2e-5, max 1.9e-4 (the largest errors sit on the repulsive wall, where
+    phi ~ R^12 amplifies the rounding of r - sigma + sigma0)."""
+    import ctypes as C
+    from parellel_mc_mpi_for_liquidcrystalsystems_b200 import _lib
+    rng = np.random.default_rng(77)
+    M = 200000
+    lp, op = params_pair(1000, 0.30, 1)
+    ei = rng.normal(size=(M, 3))
+    ej = rng.normal(size=(M, 3))
+    ei /= np.linalg.norm(ei, axis=1, keepdims=True)
+    ej /= np.linalg.norm(ej, axis=1, keepdims=True)
+    d = rng.normal(size=(M, 3))
+    d *= (rng.uniform(0.8, 4.2, size=M) / np.linalg.norm(d, axis=1))[:, None]
+    d, ei, ej = (np.ascontiguousarray(x) for x in (d, ei, ej))
+    o32 = np.zeros(M)
+    o64 = np.zeros(M)
+    _lib.check(_lib.lib().lcmc_pair_terms(C.byref(lp), M, d.ctypes.data_as(_lib.DP), ei.ctypes.data_as(_lib.DP),
+                                          ej.ctypes.data_as(_lib.DP), o32.ctypes.data_as(_lib.DP),
+                                          o64.ctypes.data_as(_lib.DP)))
+    c = oc.consts(op, oc.ARITH_CANONICAL)
+    big = np.array([1e9, 1e9, 1e9])
+    zero = np.zeros(3)
+    want = np.empty(2000)
+    for m in range(2000):
+        inc = C.c_int()
+        want[m] = oc.lib().lco_pair(C.byref(c), oc.ptr(zero), oc.ptr(np.ascontiguousarray(ei[m])),
+                                    oc.ptr(np.ascontiguousarray(d[m])), oc.ptr(np.ascontiguousarray(ej[m])),
+                                    oc.ptr(big), C.byref(inc))
+    assert np.array_equal(bits(o64[:2000]), bits(want))
+    inc = (np.sum(d * d, axis=1) < 16.0) & (o64 < 1e8)
+    err = np.abs(o32 - o64)[inc] / np.maximum(np.abs(o64[inc]), 1.0)
+    print(f"FP32 pair error over {inc.sum()} pairs: median {np.median(err):.2e}, p99 {np.quantile(err, 0.99):.2e}, "
+          f"max {err.max():.2e}")
+    assert np.median(err) < 1e-6
+    assert np.quantile(err, 0.99) < 1e-4
+    assert err.max() < 1e-3
 
 
 def test_fp32_runs_are_deterministic():
