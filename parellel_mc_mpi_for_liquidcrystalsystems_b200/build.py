@@ -25,7 +25,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 SOURCES = {
     "lcmc_sweep_exact.cu": ["-fmad=false"],
     "lcmc_sweep_fast.cu": [],
-    "lcmc_rebin.cu": [],
+    "lcmc_rebin.cu": ["-fmad=false"],  # builds the trial moves (same arithmetic as the FP64 kernel)
     "lcmc_misc.cu": ["-fmad=false"],
     "lcmc_api.cu": ["-fmad=false"],
     "lcmc_pairtest.cu": [],

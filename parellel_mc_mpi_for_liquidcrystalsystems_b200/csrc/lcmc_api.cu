@@ -44,6 +44,9 @@ struct lcmc_ctx {
     double *d_pe0 = nullptr, *d_pe1 = nullptr;
     int *d_phard = nullptr;
     double *d_red = nullptr;
+    double *d_trial_d[8] = {nullptr}; // tnx tny tnz tux tuy tuz tdU tlu
+    float *d_trial_f[3] = {nullptr};  // tdx tdy tdz
+    unsigned char *d_thard = nullptr;
     int cur = 0;
     bool uploaded_all = false;
     std::vector<char> uploaded;
@@ -414,6 +417,18 @@ static DevView view(const lcmc_ctx *c, int parity)
     v.cell_cands = c->d_cell_cands;
     v.outcome = c->d_outcome;
     v.scratch_d = c->d_red;
+    v.tnx = c->d_trial_d[0];
+    v.tny = c->d_trial_d[1];
+    v.tnz = c->d_trial_d[2];
+    v.tux = c->d_trial_d[3];
+    v.tuy = c->d_trial_d[4];
+    v.tuz = c->d_trial_d[5];
+    v.tdU = c->d_trial_d[6];
+    v.tlu = c->d_trial_d[7];
+    v.tdx = c->d_trial_f[0];
+    v.tdy = c->d_trial_f[1];
+    v.tdz = c->d_trial_f[2];
+    v.thard = c->d_thard;
     return v;
 }
 
@@ -430,6 +445,11 @@ static void free_ctx(lcmc_ctx *c)
                     c->d_pe0, c->d_pe1, c->d_phard, c->d_red};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (int k = 0; k < 8; k++)
+        if (c->d_trial_d[k]) cudaFree(c->d_trial_d[k]);
+    for (int k = 0; k < 3; k++)
+        if (c->d_trial_f[k]) cudaFree(c->d_trial_f[k]);
+    if (c->d_thard) cudaFree(c->d_thard);
     for (int a = 0; a < 2; a++)
         for (int k = 0; k < 6; k++)
             if (c->d_x[a][k]) cudaFree(c->d_x[a][k]);
@@ -458,6 +478,7 @@ static void choose_kernels(lcmc_ctx *c)
 {
     c->any_fast = c->any_exact = c->any_npt = false;
     int need_amax = 0;
+    bool spec21 = true; // every system has mu = 2, nu = 1, sigma0 = 1
     for (int r = 0; r < c->R; r++) {
         Replica &rp = c->rep[r];
         const lcmc_params &p = c->params[r];
@@ -467,17 +488,20 @@ static void choose_kernels(lcmc_ctx *c)
         if (kern == 1) {
             c->any_fast = true;
             if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
+            // active-cell capacity: mean occupancy + 12 + 50% (a dense liquid's
+            // cell counts fluctuate far less than that; overflow is flagged)
             double wcell = rp.L[0] / (double)nc;
             double mean = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]) * wcell * wcell * wcell;
-            int want = (int)(2.0 * mean + 16.0);
+            int want = (int)(1.5 * mean + 12.0);
             if (p.cell_capacity > want) want = p.cell_capacity;
             if (want > need_amax) need_amax = want;
         } else {
             c->any_exact = true;
         }
         if (rp.ensemble == 2) c->any_npt = true;
+        spec21 = spec21 && p.gb_mu_exponent == 2.0 && p.gb_nu_exponent == 1.0 && p.gb_sigma_sidetoside == 1.0;
     }
-    c->fast_variant = need_amax > 48 ? 1 : 0;
+    c->fast_variant = 2 * (need_amax > 48 ? 1 : 0) + (spec21 ? 1 : 0);
 }
 
 static int upload_replica_table(lcmc_ctx *c)
@@ -579,6 +603,9 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     ALLOC(c->d_pe1, c->ntot);
     ALLOC(c->d_phard, c->ntot);
     ALLOC(c->d_red, 16 * n + 16);
+    for (int k = 0; k < 8; k++) ALLOC(c->d_trial_d[k], c->ntot);
+    for (int k = 0; k < 3; k++) ALLOC(c->d_trial_f[k], c->ntot);
+    ALLOC(c->d_thard, c->ntot);
 #undef ALLOC
     if ((c->ctot + 4095) / 4096 > 4096) {
         free_ctx(c);
@@ -652,19 +679,21 @@ static void enqueue_rebin(lcmc_ctx *c, int parity) { launch_rebin(view(c, parity
 // time its parts on the device (lcmc_last_sweep_timing).
 static void enqueue_sweep(lcmc_ctx *c, int parity)
 {
-    cudaEventRecord(c->ev[0], c->stream);
+    // cudaEventRecordExternal: captured as event-record nodes (timestamps), not
+    // as internal dependencies
+    cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal);
     enqueue_rebin(c, parity);
-    cudaEventRecord(c->ev[1], c->stream);
+    cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal);
     DevView v = view(c, parity ^ 1);
     for (int ci = 0; ci < 8; ci++) {
         if (c->any_exact) launch_phase_exact(v, c->stream, ci, c->grid_exact);
         if (c->any_fast) launch_phase_fast(c->fast_variant, v, c->stream, ci, c->grid_fast);
     }
-    cudaEventRecord(c->ev[2], c->stream);
+    cudaEventRecordWithFlags(c->ev[2], c->stream, cudaEventRecordExternal);
     if (c->any_npt) launch_volume(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_exact);
-    cudaEventRecord(c->ev[3], c->stream);
+    cudaEventRecordWithFlags(c->ev[3], c->stream, cudaEventRecordExternal);
     launch_finalize(v, c->stream);
-    cudaEventRecord(c->ev[4], c->stream);
+    cudaEventRecordWithFlags(c->ev[4], c->stream, cudaEventRecordExternal);
 }
 
 static int check_flags(lcmc_ctx *c)

@@ -117,6 +117,36 @@ struct FastK {
     float mu, nu;
 };
 
+// mu = 2, nu = 1, sigma0 = 1 (the Gay-Berne parametrisation of every workload
+// here), without the general branches.
+__device__ __forceinline__ float pair_fast_21(const FastK &k, float dx, float dy, float dz, float r2, float eix,
+                                              float eiy, float eiz, float ejx, float ejy, float ejz)
+{
+    float ir = rsqrtf(r2);
+    float r = r2 * ir;
+    float a = (dx * eix + dy * eiy + dz * eiz) * ir;
+    float b = (dx * ejx + dy * ejy + dz * ejz) * ir;
+    float c = eix * ejx + eiy * ejy + eiz * ejz;
+    float s = a + b, d = a - b;
+    float s2 = s * s, d2 = d * d;
+    float sp = s2 + d2, sm = s2 - d2;
+    float c2 = c * c;
+    float eps1 = rsqrtf(1.0f - k.chi_sq * c2);
+    float s_chi = 1.0f - k.half_chi * (sp - k.chi * c * sm) * (eps1 * eps1);
+    float inv2 = __fdividef(1.0f, 1.0f - k.chip_sq * c2);
+    float eps2 = 1.0f - k.half_chip * (sp - k.chip * c * sm) * inv2;
+    float dr = r - rsqrtf(s_chi) + 1.0f;
+    float R = __fdividef(1.0f, dr);
+    float R2 = R * R;
+    float R6 = R2 * R2 * R2;
+    float v = k.four_eps0 * (eps1 * eps2 * eps2) * R6 * (R6 - 1.0f);
+    return dr < 0.001f ? 1.0e9f : v;
+}
+
+template <bool SPEC21>
+__device__ __forceinline__ float pair_fast_t(const FastK &k, float dx, float dy, float dz, float r2, float eix,
+                                             float eiy, float eiz, float ejx, float ejy, float ejz);
+
 __device__ __forceinline__ float pair_fast(const FastK &k, float dx, float dy, float dz, float r2, float eix,
                                            float eiy, float eiz, float ejx, float ejy, float ejz)
 {
@@ -145,4 +175,19 @@ __device__ __forceinline__ float pair_fast(const FastK &k, float dx, float dy, f
     return dr < 0.001f ? 1.0e9f : v;
 }
 
+} // namespace lcmc
+
+namespace lcmc {
+template <>
+__device__ __forceinline__ float pair_fast_t<true>(const FastK &k, float dx, float dy, float dz, float r2, float eix,
+                                                   float eiy, float eiz, float ejx, float ejy, float ejz)
+{
+    return pair_fast_21(k, dx, dy, dz, r2, eix, eiy, eiz, ejx, ejy, ejz);
+}
+template <>
+__device__ __forceinline__ float pair_fast_t<false>(const FastK &k, float dx, float dy, float dz, float r2, float eix,
+                                                    float eiy, float eiz, float ejx, float ejy, float ejz)
+{
+    return pair_fast(k, dx, dy, dz, r2, eix, eiy, eiz, ejx, ejy, ejz);
+}
 } // namespace lcmc

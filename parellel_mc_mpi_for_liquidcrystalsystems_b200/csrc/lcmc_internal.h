@@ -78,6 +78,13 @@ struct DevView {
     unsigned long long *cell_pairs, *cell_cands;
     unsigned char *outcome;    // [ntot] by particle slot of id: 0/1/2
     double *scratch_d;         // [R * 8] small reductions
+    // this sweep's trial moves, by sorted slot (FP32 kernel systems)
+    double *tnx, *tny, *tnz;   // new position, wrapped
+    double *tux, *tuy, *tuz;   // new orientation, normalised
+    double *tdU;               // colloid-term change
+    double *tlu;               // log of the Metropolis draw
+    float *tdx, *tdy, *tdz;    // displacement
+    unsigned char *thard;      // 1 = colloid hard-core reject
 };
 
 } // namespace lcmc

@@ -17,6 +17,7 @@
 
 #include "lcmc_internal.h"
 #include "lcmc_rng.cuh"
+#include "lcmc_trial.cuh"
 
 namespace lcmc {
 
@@ -216,18 +217,43 @@ __global__ void k_sort_cells(DevView v)
     }
 }
 
+// Permute into the other buffer and, for systems on the FP32 kernel, build
+// this sweep's trial move of every particle (a particle is attempted once per
+// sweep from its sweep-start state, so the trial is known now): new state,
+// displacement, colloid-term change, log of the Metropolis draw, hard-core flag.
 __global__ void k_gather(DevView v)
 {
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < v.ntot; g += gridDim.x * blockDim.x) {
         int src = v.rank[g];
-        v.qx[g] = v.px[src];
-        v.qy[g] = v.py[src];
-        v.qz[g] = v.pz[src];
-        v.qux[g] = v.ox[src];
-        v.quy[g] = v.oy[src];
-        v.quz[g] = v.oz[src];
-        v.qid[g] = v.id[src];
+        const double ro[3] = {v.px[src], v.py[src], v.pz[src]};
+        const double eo[3] = {v.ox[src], v.oy[src], v.oz[src]};
+        const int id = v.id[src];
+        v.qx[g] = ro[0];
+        v.qy[g] = ro[1];
+        v.qz[g] = ro[2];
+        v.qux[g] = eo[0];
+        v.quy[g] = eo[1];
+        v.quz[g] = eo[2];
+        v.qid[g] = id;
         v.scid[g] = v.cid[src];
+        const Replica &p = v.rep[v.p2r[g]];
+        if (!p.use_fast) continue;
+        double rn[3], en[3], dsp[3], u;
+        const int ok = make_trial(p, (uint32_t)id, ro, eo, rn, en, dsp, &u);
+        double dU = 0.0;
+        if (ok && p.k.coll_on) dU = colloid_rod(p.k, rn, en, p.L) - colloid_rod(p.k, ro, eo, p.L);
+        v.tnx[g] = rn[0];
+        v.tny[g] = rn[1];
+        v.tnz[g] = rn[2];
+        v.tux[g] = en[0];
+        v.tuy[g] = en[1];
+        v.tuz[g] = en[2];
+        v.tdx[g] = (float)dsp[0];
+        v.tdy[g] = (float)dsp[1];
+        v.tdz[g] = (float)dsp[2];
+        v.tdU[g] = dU;
+        v.tlu[g] = log_unit(u);
+        v.thard[g] = (unsigned char)!ok;
     }
 }
 

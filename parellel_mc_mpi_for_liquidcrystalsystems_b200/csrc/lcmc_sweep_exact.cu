@@ -16,6 +16,7 @@
 #include "lcmc_gb.cuh"
 #include "lcmc_internal.h"
 #include "lcmc_rng.cuh"
+#include "lcmc_trial.cuh"
 
 namespace lcmc {
 
@@ -35,51 +36,6 @@ __device__ __forceinline__ double warp_sum_butterfly(double x)
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) x = x + __shfl_xor_sync(0xffffffffu, x, o);
     return x;
-}
-
-// apply_pbc (MCnptColloid.c:2420-2430)
-__device__ __forceinline__ void apply_pbc(double r[3], const double L[3])
-{
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        if (r[a] > L[a]) r[a] -= L[a];
-        else if (r[a] < 0.0) r[a] += L[a];
-    }
-}
-
-// Trial move of one particle (MCnptColloid.c:2502-2551 with Philox draws):
-// returns 0 if the colloid hard core rejects it (no energy evaluation).
-__device__ __forceinline__ int make_trial(const Replica &p, uint32_t id, const double ro[3], const double eo[3],
-                                          double rn[3], double en[3], double *u_acc)
-{
-    U4 m = draw(p.key, id, p.sweep, TAG_MOVE);
-    const double d = p.k.max_disp;
-    rn[0] = ro[0] + d * (u01(m.x) - 0.5);
-    rn[1] = ro[1] + d * (u01(m.y) - 0.5);
-    rn[2] = ro[2] + d * (u01(m.z) - 0.5);
-    *u_acc = u01(m.w);
-    apply_pbc(rn, p.L);
-    double c[3];
-    double r2 = dist_fold(rn[0], rn[1], rn[2], 0.5 * p.L[0], 0.5 * p.L[1], 0.5 * p.L[2], p.L, c);
-    if (!(r2 > p.k.coll_R * p.k.coll_R)) return 0;
-    double v[3];
-    sphere_point(p.key, id, p.sweep, v);
-    const double a = p.k.max_rot;
-    en[0] = a * v[0] + eo[0];
-    en[1] = a * v[1] + eo[1];
-    en[2] = a * v[2] + eo[2];
-    double n2 = en[0] * en[0] + en[1] * en[1] + en[2] * en[2];
-    if (n2 <= 1e-12) {
-        en[0] = eo[0];
-        en[1] = eo[1];
-        en[2] = eo[2];
-    } else {
-        double nr = __dsqrt_rn(n2);
-        en[0] /= nr;
-        en[1] /= nr;
-        en[2] /= nr;
-    }
-    return 1;
 }
 
 __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
@@ -142,8 +98,8 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
             const uint32_t id = (uint32_t)v.id[g];
             double ro[3] = {v.px[g], v.py[g], v.pz[g]};
             double eo[3] = {v.ox[g], v.oy[g], v.oz[g]};
-            double rn[3], en[3], uacc;
-            int ok = make_trial(p, id, ro, eo, rn, en, &uacc);
+            double rn[3], en[3], dsp[3], uacc;
+            int ok = make_trial(p, id, ro, eo, rn, en, dsp, &uacc);
             if (!ok) {
                 if (lane == 0) v.outcome[p.p_off + id] = 2;
                 nhard++;

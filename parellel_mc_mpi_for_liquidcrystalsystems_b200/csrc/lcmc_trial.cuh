@@ -1,0 +1,66 @@
+// lcmc_trial.cuh - the trial move of one particle (translation + rotation).
+#pragma once
+#include "lcmc_gb.cuh"
+#include "lcmc_internal.h"
+#include "lcmc_rng.cuh"
+
+namespace lcmc {
+
+// apply_pbc (MCnptColloid.c:2420-2430): a single +-L fold per axis.
+__device__ __forceinline__ void apply_pbc(double r[3], const double L[3])
+{
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (r[a] > L[a]) r[a] -= L[a];
+        else if (r[a] < 0.0) r[a] += L[a];
+    }
+}
+
+// Trial move of attempt_monte_carlo_move (MCnptColloid.c:2502-2551) with
+// Philox draws in place of rand():
+//   r' = r + d (u - 1/2) per axis (d = max_displacement, full width), wrapped;
+//   colloid hard core: reject without energy evaluation if |r' - C|^2 <= R^2;
+//   u' = normalise(u + max_rotation v), v a Marsaglia point on the sphere;
+//        the old orientation is kept if |u + max_rotation v|^2 <= 1e-12.
+// Returns 0 on a hard-core reject (en = eo then).  dsp receives the
+// unwrapped displacement, *u_acc the Metropolis draw.
+__device__ __forceinline__ int make_trial(const Replica &p, uint32_t id, const double ro[3], const double eo[3],
+                                          double rn[3], double en[3], double dsp[3], double *u_acc)
+{
+    U4 m = draw(p.key, id, p.sweep, TAG_MOVE);
+    const double d = p.k.max_disp;
+    dsp[0] = d * (u01(m.x) - 0.5);
+    dsp[1] = d * (u01(m.y) - 0.5);
+    dsp[2] = d * (u01(m.z) - 0.5);
+    rn[0] = ro[0] + dsp[0];
+    rn[1] = ro[1] + dsp[1];
+    rn[2] = ro[2] + dsp[2];
+    *u_acc = u01(m.w);
+    apply_pbc(rn, p.L);
+    en[0] = eo[0];
+    en[1] = eo[1];
+    en[2] = eo[2];
+    double c[3];
+    double r2 = dist_fold(rn[0], rn[1], rn[2], 0.5 * p.L[0], 0.5 * p.L[1], 0.5 * p.L[2], p.L, c);
+    if (!(r2 > p.k.coll_R * p.k.coll_R)) return 0;
+    double v[3];
+    sphere_point(p.key, id, p.sweep, v);
+    const double a = p.k.max_rot;
+    en[0] = a * v[0] + eo[0];
+    en[1] = a * v[1] + eo[1];
+    en[2] = a * v[2] + eo[2];
+    double n2 = en[0] * en[0] + en[1] * en[1] + en[2] * en[2];
+    if (n2 <= 1e-12) {
+        en[0] = eo[0];
+        en[1] = eo[1];
+        en[2] = eo[2];
+    } else {
+        double nr = __dsqrt_rn(n2);
+        en[0] /= nr;
+        en[1] /= nr;
+        en[2] /= nr;
+    }
+    return 1;
+}
+
+} // namespace lcmc
