@@ -183,6 +183,31 @@ int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4]);
 int lcmc_pair_terms(const lcmc_params *p, int n, const double *d, const double *ei, const double *ej, double *out32,
                     double *out64);
 
+/* ---- allocation-free total energy (no counterpart in the reference) ----
+ * Some callers cannot let this library allocate device memory: a host program
+ * that has already reserved the GPU's memory for its own pool, or a time-step
+ * loop that cannot afford the device-wide synchronisation cudaMalloc/cudaFree
+ * imply.  For them this call computes the FP64 total energy (what tot_ene
+ * computes) of a configuration the caller already holds in device memory, using
+ * only a fixed scratch area compiled into liblcmc.so (1.7 MB on every GPU that
+ * loads the library, held until the process exits).
+ *   d_px..d_oz  device arrays of n doubles (positions in [0, L], orientations)
+ *   box         host array, box edges; cells of width >= cutoff_radius
+ *   d_energy    device pointer receiving the energy
+ *   stream      cudaStream_t to enqueue on (NULL = legacy default stream)
+ * Limits: n <= LCMC_NOALLOC_MAX_PARTICLES and (L/rc) cells per axis with at most
+ * LCMC_NOALLOC_MAX_CELLS cells in total; larger inputs return LCMC_EINVAL with a
+ * message (lcmc_last_error(NULL, ...)).  Asynchronous: synchronise the stream
+ * before reading d_energy.  The first call on a device looks up the scratch
+ * area's device address; make that first call before any stream capture.  All
+ * calls share the one scratch area: calls that overlap on the GPU (other
+ * streams, other host threads) race and give wrong results. */
+#define LCMC_NOALLOC_MAX_PARTICLES 65536
+#define LCMC_NOALLOC_MAX_CELLS 32768
+int lcmc_total_energy_noalloc(const lcmc_params *p, int n, const double *d_px, const double *d_py, const double *d_pz,
+                              const double *d_ox, const double *d_oy, const double *d_oz, const double box[3],
+                              double *d_energy, void *stream);
+
 const char *lcmc_strerror(int code);
 /* Last error message of this context (or of the last failed create when ctx is NULL). */
 int lcmc_last_error(const lcmc_ctx *ctx, char *buf, size_t len);

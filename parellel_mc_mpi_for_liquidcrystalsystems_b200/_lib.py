@@ -79,6 +79,8 @@ EXPORTS = {
     "lcmc_kernels_per_sweep": ([C.c_void_p], C.c_int),
     "lcmc_last_sweep_timing": ([C.c_void_p, DP], C.c_int),
     "lcmc_pair_terms": ([C.POINTER(Params), C.c_int, DP, DP, DP, DP, DP], C.c_int),
+    "lcmc_total_energy_noalloc": ([C.POINTER(Params), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, DP, C.c_void_p, C.c_void_p], C.c_int),
 }
 
 

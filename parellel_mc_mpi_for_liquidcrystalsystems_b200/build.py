@@ -30,6 +30,7 @@ SOURCES = {
     "lcmc_api.cu": ["-fmad=false"],
     "lcmc_pairtest.cu": [],
     "lcmc_pairtest64.cu": ["-fmad=false"],
+    "lcmc_noalloc.cu": ["-fmad=false"],
 }
 
 

@@ -765,6 +765,25 @@ extern "C" int lcmc_pair_terms(const lcmc_params *p, int n, const double *d, con
     return LCMC_OK;
 }
 
+// Allocation-free total energy: no counterpart in the reference; for callers
+// that must not let this library allocate device memory (see lcmc.h).  Makes
+// no cudaMalloc/cudaFree call; scratch is the fixed area in lcmc_noalloc.cu.
+extern "C" int lcmc_total_energy_noalloc(const lcmc_params *p, int n, const double *d_px, const double *d_py,
+                                         const double *d_pz, const double *d_ox, const double *d_oy,
+                                         const double *d_oz, const double box[3], double *d_energy, void *stream)
+{
+    if (!p || n < 0 || !box || !d_energy || (n > 0 && (!d_px || !d_py || !d_pz || !d_ox || !d_oy || !d_oz)))
+        return set_err(nullptr, LCMC_EINVAL, "bad arguments");
+    if (p->cutoff_radius <= 0.0) return set_err(nullptr, LCMC_EINVAL, "cutoff_radius must be positive");
+    GBConsts k;
+    make_consts(*p, k);
+    char msg[256] = {0};
+    int rc = total_energy_noalloc(k, n, d_px, d_py, d_pz, d_ox, d_oy, d_oz, box, d_energy, (cudaStream_t)stream, msg,
+                                  sizeof(msg));
+    if (rc) return set_err(nullptr, rc, msg);
+    return LCMC_OK;
+}
+
 extern "C" int lcmc_get_stream(lcmc_ctx *ctx, void **stream)
 {
     if (!ctx || !stream) return LCMC_EINVAL;

@@ -29,6 +29,11 @@ void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int
 void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out);
 void launch_to_id_order(const DevView &v, cudaStream_t s, int r, int grid);
 
+// lcmc_noalloc.cu (allocation-free FP64 total energy on a caller's stream)
+int total_energy_noalloc(const GBConsts &k, int n, const double *px, const double *py, const double *pz,
+                         const double *ox, const double *oy, const double *oz, const double box[3], double *d_out,
+                         cudaStream_t st, char *msg, size_t len);
+
 // lcmc_pairtest.cu / lcmc_pairtest64.cu (pair term on given inputs)
 void launch_pair_terms32(const GBConsts &k, int n, const double *d, const double *ei, const double *ej, double *out,
                          cudaStream_t s);
