@@ -44,7 +44,8 @@ enum {
     LCMC_ENUMERIC = -7,  /* NaN or Inf energy */
     LCMC_EBOX = -8,      /* box too small for the cutoff (L < 2 rc) or inconsistent sizes */
     LCMC_ENODEV = -9,    /* no CUDA device */
-    LCMC_EOVERLAP = -10  /* a particle centre inside the colloid (check_no_colloid_overlaps, MCnptColloid.c:1324-1340) */
+    LCMC_EOVERLAP = -10, /* a particle centre inside the colloid (check_no_colloid_overlaps, MCnptColloid.c:1324-1340) */
+    LCMC_ETIMEOUT = -11  /* a bounded wait inside a tensor-core kernel gave up (the kernel returned cleanly) */
 };
 
 enum { LCMC_PREC_FP64 = 0, LCMC_PREC_FP32 = 1 };
@@ -182,6 +183,28 @@ int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4]);
  * Pairs beyond the cutoff give 0.  For tests and error statistics. */
 int lcmc_pair_terms(const lcmc_params *p, int n, const double *d, const double *ei, const double *ej, double *out32,
                     double *out64);
+
+/* ---- learned volume-move surrogate (no counterpart in the reference, which has
+ *      no NPT move: system_pressure is parsed at MCnptColloid.c:3978 and unused) ----
+ * An MLP n_in -> 128 -> 128 -> 1 (SiLU), BF16 weights and activations, FP32
+ * accumulation; its matrix products run on the tensor cores (tcgen05). */
+typedef struct lcmc_mlp lcmc_mlp;
+int lcmc_mlp_create(int n_in, int hidden, int max_batch, uint64_t seed, lcmc_mlp **out);
+int lcmc_mlp_destroy(lcmc_mlp *m);
+/* Adam on mean squared error; x: n rows of n_in floats, t: n targets (host). */
+int lcmc_mlp_train(lcmc_mlp *m, const float *x, const float *t, int n, int epochs, int batch, float lr, uint64_t seed,
+                   float *final_loss);
+int lcmc_mlp_predict(lcmc_mlp *m, const float *x, int n, float *y);
+/* Gradient of the batch MSE w.r.t. all parameters without updating them, and
+ * parameter get/set (layout: W1 [128 x k1] | b1 | W2 [128 x 128] | b2 | w3 | b3,
+ * k1 = n_in rounded up to 128); for gradient checks. */
+int lcmc_mlp_num_params(const lcmc_mlp *m);
+int lcmc_mlp_gradients(lcmc_mlp *m, const float *x, const float *t, int n, float *grad, float *loss);
+int lcmc_mlp_get_params(lcmc_mlp *m, float *params);
+int lcmc_mlp_set_params(lcmc_mlp *m, const float *params);
+/* C[M x N] = A[M x K] B[N x K]^T with A, B rounded to BF16, FP32 accumulate, on
+ * the tensor cores (host arrays; K a multiple of 64).  For tests. */
+int lcmc_gemm_bf16(const float *A, const float *B, float *C, int M, int N, int K);
 
 /* ---- allocation-free total energy (no counterpart in the reference) ----
  * Some callers cannot let this library allocate device memory: a host program

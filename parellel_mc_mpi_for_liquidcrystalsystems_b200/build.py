@@ -31,6 +31,7 @@ SOURCES = {
     "lcmc_pairtest.cu": [],
     "lcmc_pairtest64.cu": ["-fmad=false"],
     "lcmc_noalloc.cu": ["-fmad=false"],
+    "lcmc_mlp.cu": [],
 }
 
 
