@@ -106,6 +106,7 @@ typedef struct {
     int64_t stencil_candidates;  /* sum over attempts of 27-cell stencil candidates, excluding self */
     int error_flags;             /* LCMC_F* bits seen by the kernels */
     int kernel;                  /* 0 = FP64 kernel, 1 = FP32 kernel */
+    int64_t volume_stage1_rejected; /* volume moves the surrogate rejected (no exact energy computed) */
 } lcmc_stats;
 
 /* error_flags bits */
@@ -205,6 +206,26 @@ int lcmc_mlp_set_params(lcmc_mlp *m, const float *params);
 /* C[M x N] = A[M x K] B[N x K]^T with A, B rounded to BF16, FP32 accumulate, on
  * the tensor cores (host arrays; K a multiple of 64).  For tests. */
 int lcmc_gemm_bf16(const float *A, const float *B, float *C, int M, int N, int K);
+
+/* Delayed-acceptance volume moves (Christen & Fox 2005) for the NPT replicas of
+ * a context: stage 1 tests the surrogate's antisymmetric energy change
+ *   dU~ = N s [g(phi(x), delta) - g(phi(y), -delta)] / 2
+ * (features phi: density, Q tensor and radial alignment on an 8^3 grid, 4097
+ * inputs with delta ln V), and only moves that pass it get the exact FP64
+ * recompute and stage 2, exp(-beta (dU - dU~)).  s = target_scale converts the
+ * network output to dU / N.  m = NULL switches it off.  The network must stay
+ * alive while set. */
+int lcmc_set_surrogate(lcmc_ctx *ctx, lcmc_mlp *m, double target_scale);
+#define LCMC_FEATURES 4097
+/* Record (features of x, exact dU / N) of every exactly evaluated volume move
+ * (capacity samples; 0 stops and frees); fetch them (x: n x 4097). */
+int lcmc_record_volume_samples(lcmc_ctx *ctx, int capacity);
+int lcmc_get_volume_samples(lcmc_ctx *ctx, float *x, float *y, int max_n);
+/* Per-sweep history (last `capacity` sweeps): rows of 9 doubles = sweep,
+ * sums of ux ux, ux uy, ux uz, uy uy, uy uz, uz uz, energy, volume.
+ * lcmc_get_history returns the number of rows written, in sweep order. */
+int lcmc_record_history(lcmc_ctx *ctx, int capacity);
+int lcmc_get_history(lcmc_ctx *ctx, int replica, double *rows, int max_rows);
 
 /* ---- allocation-free total energy (no counterpart in the reference) ----
  * Some callers cannot let this library allocate device memory: a host program

@@ -17,6 +17,8 @@ NVT, NPT = 1, 2
 
 D = C.c_double
 DP = C.POINTER(C.c_double)
+FP = C.POINTER(C.c_float)
+N_FEATURES = 4097
 
 
 class Params(C.Structure):
@@ -43,7 +45,7 @@ class Stats(C.Structure):
         ("sweeps", C.c_int64), ("attempted", C.c_int64), ("accepted", C.c_int64), ("hardcore_rejected", C.c_int64),
         ("volume_attempted", C.c_int64), ("volume_accepted", C.c_int64), ("energy", D), ("box", D * 3),
         ("last_recompute", D), ("drift", D), ("pairs_in_cutoff", C.c_int64), ("stencil_candidates", C.c_int64),
-        ("error_flags", C.c_int), ("kernel", C.c_int),
+        ("error_flags", C.c_int), ("kernel", C.c_int), ("volume_stage1_rejected", C.c_int64),
     ]
 
 
@@ -81,6 +83,20 @@ EXPORTS = {
     "lcmc_pair_terms": ([C.POINTER(Params), C.c_int, DP, DP, DP, DP, DP], C.c_int),
     "lcmc_total_energy_noalloc": ([C.POINTER(Params), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, DP, C.c_void_p, C.c_void_p], C.c_int),
+    "lcmc_mlp_create": ([C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
+    "lcmc_mlp_destroy": ([C.c_void_p], C.c_int),
+    "lcmc_mlp_train": ([C.c_void_p, FP, FP, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64, FP], C.c_int),
+    "lcmc_mlp_predict": ([C.c_void_p, FP, C.c_int, FP], C.c_int),
+    "lcmc_mlp_num_params": ([C.c_void_p], C.c_int),
+    "lcmc_mlp_gradients": ([C.c_void_p, FP, FP, C.c_int, FP, FP], C.c_int),
+    "lcmc_mlp_get_params": ([C.c_void_p, FP], C.c_int),
+    "lcmc_mlp_set_params": ([C.c_void_p, FP], C.c_int),
+    "lcmc_gemm_bf16": ([FP, FP, FP, C.c_int, C.c_int, C.c_int], C.c_int),
+    "lcmc_set_surrogate": ([C.c_void_p, C.c_void_p, C.c_double], C.c_int),
+    "lcmc_record_volume_samples": ([C.c_void_p, C.c_int], C.c_int),
+    "lcmc_get_volume_samples": ([C.c_void_p, FP, FP, C.c_int], C.c_int),
+    "lcmc_record_history": ([C.c_void_p, C.c_int], C.c_int),
+    "lcmc_get_history": ([C.c_void_p, C.c_int, DP, C.c_int], C.c_int),
 }
 
 

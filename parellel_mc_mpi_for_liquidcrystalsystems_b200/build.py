@@ -32,6 +32,7 @@ SOURCES = {
     "lcmc_pairtest64.cu": ["-fmad=false"],
     "lcmc_noalloc.cu": ["-fmad=false"],
     "lcmc_mlp.cu": [],
+    "lcmc_da.cu": [],
 }
 
 

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/lcmc.h"
@@ -47,6 +48,16 @@ struct lcmc_ctx {
     double *d_trial_d[8] = {nullptr}; // tnx tny tnz tux tuy tuz tdU tlu
     float *d_trial_f[3] = {nullptr};  // tdx tdy tdz
     unsigned char *d_thard = nullptr;
+    // surrogate, recordings
+    unsigned long long *d_feat_acc = nullptr;
+    float *d_feat_f = nullptr;
+    int rec_cap = 0;
+    int *d_rec_count = nullptr;
+    float *d_rec_x = nullptr, *d_rec_y = nullptr;
+    int hist_cap = 0;
+    double *d_hist = nullptr;
+    lcmc_mlp *mlp = nullptr;
+    bool any_da = false;
     int cur = 0;
     bool uploaded_all = false;
     std::vector<char> uploaded;
@@ -429,6 +440,14 @@ static DevView view(const lcmc_ctx *c, int parity)
     v.tdy = c->d_trial_f[1];
     v.tdz = c->d_trial_f[2];
     v.thard = c->d_thard;
+    v.feat_acc = c->d_feat_acc;
+    v.feat_f = c->d_feat_f;
+    v.rec_cap = c->rec_cap;
+    v.rec_count = c->d_rec_count;
+    v.rec_x = c->d_rec_x;
+    v.rec_y = c->d_rec_y;
+    v.hist_cap = c->hist_cap;
+    v.hist = c->d_hist;
     return v;
 }
 
@@ -450,6 +469,9 @@ static void free_ctx(lcmc_ctx *c)
     for (int k = 0; k < 3; k++)
         if (c->d_trial_f[k]) cudaFree(c->d_trial_f[k]);
     if (c->d_thard) cudaFree(c->d_thard);
+    void *more[] = {c->d_feat_acc, c->d_feat_f, c->d_rec_count, c->d_rec_x, c->d_rec_y, c->d_hist};
+    for (void *p : more)
+        if (p) cudaFree(p);
     for (int a = 0; a < 2; a++)
         for (int k = 0; k < 6; k++)
             if (c->d_x[a][k]) cudaFree(c->d_x[a][k]);
@@ -606,6 +628,8 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     for (int k = 0; k < 8; k++) ALLOC(c->d_trial_d[k], c->ntot);
     for (int k = 0; k < 3; k++) ALLOC(c->d_trial_f[k], c->ntot);
     ALLOC(c->d_thard, c->ntot);
+    ALLOC(c->d_feat_acc, (size_t)n * 512 * 7);
+    ALLOC(c->d_feat_f, (size_t)n * LCMC_FEAT);
 #undef ALLOC
     if ((c->ctot + 4095) / 4096 > 4096) {
         free_ctx(c);
@@ -690,9 +714,21 @@ static void enqueue_sweep(lcmc_ctx *c, int parity)
         if (c->any_fast) launch_phase_fast(c->fast_variant, v, c->stream, ci, c->grid_fast);
     }
     cudaEventRecordWithFlags(c->ev[2], c->stream, cudaEventRecordExternal);
-    if (c->any_npt) launch_volume(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_exact);
+    if (c->any_npt) {
+        launch_volume_propose(v, c->stream);
+        if (c->any_da || c->rec_cap > 0)
+            launch_features(v, c->stream, c->any_da ? mlp_input(c->mlp) : nullptr, c->any_da ? mlp_ld(c->mlp) : 0,
+                            c->grid_elem);
+        if (c->any_da) {
+            const int B = (2 * c->R + 127) / 128 * 128;
+            const float *y = mlp_forward_device(c->mlp, B, c->stream);
+            launch_da_stage1(v, c->stream, y);
+        }
+        launch_volume_finish(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_exact);
+    }
     cudaEventRecordWithFlags(c->ev[3], c->stream, cudaEventRecordExternal);
     launch_finalize(v, c->stream);
+    if (c->hist_cap > 0) launch_hist_record(v, c->stream);
     cudaEventRecordWithFlags(c->ev[4], c->stream, cudaEventRecordExternal);
 }
 
@@ -794,8 +830,115 @@ extern "C" int lcmc_get_stream(lcmc_ctx *ctx, void **stream)
 extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
 {
     if (!ctx) return LCMC_EINVAL;
-    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases; volume: propose, energy, accept, scale; finalize
-    return 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 4 * (int)ctx->any_npt + 1;
+    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases; volume: propose, energy, accept, scale;
+    // surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1; recording; history; finalize
+    int n = 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 4 * (int)ctx->any_npt + 1;
+    if (ctx->any_npt && (ctx->any_da || ctx->rec_cap > 0)) n += 2;
+    if (ctx->any_npt && ctx->any_da) n += 6;
+    if (ctx->any_npt && ctx->rec_cap > 0) n += 1;
+    if (ctx->hist_cap > 0) n += 1;
+    return n;
+}
+
+static int push_replica_fields(lcmc_ctx *c, int r)
+{
+    Replica &rp = c->rep[r];
+    char *base = (char *)c->d_rep + sizeof(Replica) * r;
+    CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, da_on), &rp.da_on, sizeof(int), cudaMemcpyHostToDevice,
+                                c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, da_scale), &rp.da_scale, sizeof(double),
+                                cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_set_surrogate(lcmc_ctx *ctx, lcmc_mlp *m, double target_scale)
+{
+    if (!ctx) return LCMC_EINVAL;
+    if (m && (mlp_n_in(m) != LCMC_FEAT || mlp_bmax(m) < 2 * ctx->R))
+        return set_err(ctx, LCMC_EINVAL, "surrogate needs 4097 inputs and a batch of at least 2 x replicas");
+    ctx->mlp = m;
+    ctx->any_da = false;
+    for (int r = 0; r < ctx->R; r++) {
+        Replica &rp = ctx->rep[r];
+        rp.da_on = (m && rp.ensemble == 2) ? 1 : 0;
+        rp.da_scale = target_scale;
+        ctx->any_da = ctx->any_da || rp.da_on;
+        int rc = push_replica_fields(ctx, r);
+        if (rc) return rc;
+    }
+    invalidate_graphs(ctx);
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_record_volume_samples(lcmc_ctx *ctx, int capacity)
+{
+    if (!ctx || capacity < 0) return LCMC_EINVAL;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->d_rec_x) cudaFree(ctx->d_rec_x);
+    if (ctx->d_rec_y) cudaFree(ctx->d_rec_y);
+    if (ctx->d_rec_count) cudaFree(ctx->d_rec_count);
+    ctx->d_rec_x = nullptr;
+    ctx->d_rec_y = nullptr;
+    ctx->d_rec_count = nullptr;
+    ctx->rec_cap = 0;
+    if (capacity > 0) {
+        CUDA_TRY(ctx, cudaMalloc(&ctx->d_rec_x, sizeof(float) * (size_t)capacity * LCMC_FEAT));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->d_rec_y, sizeof(float) * (size_t)capacity));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->d_rec_count, sizeof(int)));
+        CUDA_TRY(ctx, cudaMemset(ctx->d_rec_count, 0, sizeof(int)));
+        ctx->rec_cap = capacity;
+    }
+    invalidate_graphs(ctx);
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_get_volume_samples(lcmc_ctx *ctx, float *x, float *y, int max_n)
+{
+    if (!ctx || max_n < 0) return LCMC_EINVAL;
+    if (!ctx->rec_cap) return 0;
+    int n = 0;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(&n, ctx->d_rec_count, sizeof(int), cudaMemcpyDeviceToHost));
+    if (n > ctx->rec_cap) n = ctx->rec_cap;
+    if (n > max_n) n = max_n;
+    if (n > 0 && x) CUDA_TRY(ctx, cudaMemcpy(x, ctx->d_rec_x, sizeof(float) * (size_t)n * LCMC_FEAT, cudaMemcpyDeviceToHost));
+    if (n > 0 && y) CUDA_TRY(ctx, cudaMemcpy(y, ctx->d_rec_y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
+    return n;
+}
+
+extern "C" int lcmc_record_history(lcmc_ctx *ctx, int capacity)
+{
+    if (!ctx || capacity < 0) return LCMC_EINVAL;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->d_hist) cudaFree(ctx->d_hist);
+    ctx->d_hist = nullptr;
+    ctx->hist_cap = 0;
+    if (capacity > 0) {
+        CUDA_TRY(ctx, cudaMalloc(&ctx->d_hist, sizeof(double) * 9 * (size_t)capacity * ctx->R));
+        CUDA_TRY(ctx, cudaMemset(ctx->d_hist, 0xFF, sizeof(double) * 9 * (size_t)capacity * ctx->R));
+        ctx->hist_cap = capacity;
+    }
+    invalidate_graphs(ctx);
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_get_history(lcmc_ctx *ctx, int replica, double *rows, int max_rows)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !rows || max_rows < 0) return LCMC_EINVAL;
+    if (!ctx->hist_cap) return 0;
+    std::vector<double> h((size_t)9 * ctx->hist_cap);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(h.data(), ctx->d_hist + (size_t)9 * ctx->hist_cap * replica,
+                             sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+    // rows in sweep order; unwritten rows hold NaN (0xFF bytes)
+    std::vector<std::pair<double, int>> order;
+    for (int i = 0; i < ctx->hist_cap; i++)
+        if (h[(size_t)9 * i] == h[(size_t)9 * i]) order.push_back({h[(size_t)9 * i], i});
+    std::sort(order.begin(), order.end());
+    int n = (int)order.size() < max_rows ? (int)order.size() : max_rows;
+    for (int k = 0; k < n; k++) memcpy(rows + (size_t)9 * k, &h[(size_t)9 * order[k].second], 9 * sizeof(double));
+    return n;
 }
 
 extern "C" int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4])
@@ -940,6 +1083,7 @@ extern "C" int lcmc_get_stats(lcmc_ctx *ctx, int replica, lcmc_stats *out)
     out->pairs_in_cutoff = (int64_t)s.pairs;
     out->stencil_candidates = (int64_t)s.cands;
     out->error_flags = s.flags;
+    out->volume_stage1_rejected = (int64_t)s.vol_s1rej;
     out->kernel = rp.use_fast;
     return LCMC_OK;
 }

@@ -37,12 +37,19 @@ struct Replica {
     int use_fast;  // this sweep runs the FP32 kernel (needs >= 4 cells per axis)
     // volume move of this sweep
     double vol_delta, vol_lambda, vol_U_old, vol_U_new;
-    int vol_state; // 0 none, 1 accepted, 2 rejected, 3 hard-core reject
+    int vol_state; // 0 none, 1 accepted, 2 rejected, 3 hard-core reject, 4 rejected by the surrogate (stage 1)
+    // delayed acceptance with the learned surrogate
+    int da_on;
+    int vol_stage1;    // 1 = the exact stage runs this sweep
+    double da_scale;   // surrogate output -> dU / N
+    double vol_dU_sur; // surrogate dU of this sweep's move
 };
+
+constexpr int LCMC_FEAT = 8 * 512 + 1; // surrogate input: 8 channels x 8^3 cells + delta ln V
 
 // Per-replica counters kept on the device.
 struct DevStats {
-    unsigned long long attempted, accepted, hard, vol_att, vol_acc, pairs, cands;
+    unsigned long long attempted, accepted, hard, vol_att, vol_acc, pairs, cands, vol_s1rej;
     double energy, last_recompute, drift;
     int flags;
     int pad;
@@ -85,6 +92,14 @@ struct DevView {
     double *tlu;               // log of the Metropolis draw
     float *tdx, *tdy, *tdz;    // displacement
     unsigned char *thard;      // 1 = colloid hard-core reject
+    // surrogate features and recordings
+    unsigned long long *feat_acc; // [R x 512 x 7] pooled sums, fixed point 2^-32
+    float *feat_f;             // [R x LCMC_FEAT] features of the current configuration
+    int rec_cap;               // sample ring capacity (0 = off)
+    int *rec_count;
+    float *rec_x, *rec_y;      // [rec_cap x LCMC_FEAT], [rec_cap]
+    int hist_cap;              // per-sweep history capacity (0 = off)
+    double *hist;              // [R x hist_cap x 9]
 };
 
 } // namespace lcmc

@@ -29,6 +29,25 @@ void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int
 void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out);
 void launch_to_id_order(const DevView &v, cudaStream_t s, int r, int grid);
 
+} // namespace lcmc
+struct lcmc_mlp;
+namespace lcmc {
+// lcmc_mlp.cu (in-sweep surrogate inference)
+void *mlp_input(lcmc_mlp *m);
+int mlp_ld(lcmc_mlp *m);
+int mlp_bmax(lcmc_mlp *m);
+int mlp_n_in(lcmc_mlp *m);
+const float *mlp_forward_device(lcmc_mlp *m, int B, cudaStream_t s);
+int *mlp_err(lcmc_mlp *m);
+
+// lcmc_da.cu (surrogate features, delayed acceptance, recordings)
+void launch_features(const DevView &v, cudaStream_t s, void *X, int ldx, int grid);
+void launch_da_stage1(const DevView &v, cudaStream_t s, const float *y);
+void launch_record_samples(const DevView &v, cudaStream_t s);
+void launch_hist_record(const DevView &v, cudaStream_t s);
+void launch_volume_propose(const DevView &v, cudaStream_t s);
+void launch_volume_finish(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid);
+
 // lcmc_noalloc.cu (allocation-free FP64 total energy on a caller's stream)
 int total_energy_noalloc(const GBConsts &k, int n, const double *px, const double *py, const double *pz,
                          const double *ox, const double *oy, const double *oz, const double box[3], double *d_out,

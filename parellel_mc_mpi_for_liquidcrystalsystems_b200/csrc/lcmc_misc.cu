@@ -55,6 +55,8 @@ __global__ void k_volume_propose(DevView v)
         U4 o = draw(p.key, SWEEP_ID, p.sweep, TAG_VOLUME);
         p.vol_delta = p.dlnv_max * (2.0 * u01(o.x) - 1.0);
         p.vol_lambda = 1.0 + expm1_small(p.vol_delta / 3.0);
+        p.vol_stage1 = 1; // the surrogate's stage 1 may clear it
+        p.vol_dU_sur = 0.0;
     }
 }
 
@@ -66,6 +68,14 @@ __global__ void k_volume_accept(DevView v, const double *e0, const double *e1, c
     const int r = blockIdx.x;
     Replica &p = v.rep[r];
     if (p.ensemble != 2) return;
+    if (p.da_on && !p.vol_stage1) { // rejected by the surrogate: no exact energy was computed
+        if (threadIdx.x == 0) {
+            v.stats[r].vol_att += 1ull;
+            v.stats[r].vol_s1rej += 1ull;
+            p.vol_state = 4;
+        }
+        return;
+    }
     __shared__ double sh[256];
     __shared__ int shi[256];
     double a = 0.0, b = 0.0;
@@ -88,6 +98,10 @@ __global__ void k_volume_accept(DevView v, const double *e0, const double *e1, c
         int state;
         if (H) {
             state = 3;
+        } else if (p.da_on) { // stage 2 of delayed acceptance: exact dU against the surrogate's
+            const double lnA2 = -p.k.beta * ((U1 - U0) - p.vol_dU_sur);
+            U4 o = draw(p.key, SWEEP_ID, p.sweep, TAG_VOLUME);
+            state = (lnA2 >= 0.0 || log_unit(u01(o.w)) <= lnA2) ? 1 : 2;
         } else {
             const double V = p.L[0] * p.L[1] * p.L[2];
             const double dV = V * expm1_small(p.vol_delta);
@@ -171,9 +185,20 @@ void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, in
 
 void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid)
 {
-    k_volume_propose<<<1, 256, 0, s>>>(v);
+    launch_volume_propose(v, s);
+    launch_volume_finish(v, s, e0, e1, hard, grid);
+}
+
+void launch_volume_propose(const DevView &v, cudaStream_t s) { k_volume_propose<<<1, 256, 0, s>>>(v); }
+
+// exact FP64 energies of the current and the scaled configuration (skipped for
+// replicas the surrogate screened out), the acceptance test, optional sample
+// recording, and the scaling of accepted replicas.
+void launch_volume_finish(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid)
+{
     launch_energy_exact(v, s, e0, e1, hard, 1, grid);
     k_volume_accept<<<v.R, 256, 0, s>>>(v, e0, e1, hard);
+    if (v.rec_cap > 0) launch_record_samples(v, s);
     k_volume_scale<<<grid, 256, 0, s>>>(v);
 }
 

@@ -377,11 +377,11 @@ extern "C" int lcmc_mlp_create(int n_in, int hidden, int max_batch, uint64_t see
     const size_t o3 = o2 + (size_t)H * H + H;
     for (int h = 0; h < H; h++) host[o3 + h] = uni(o3 + h, a3);
     cudaMemcpy(m->P, host.data(), m->np * 4, cudaMemcpyHostToDevice);
-    cudaMemset(m->Mm, 0, m->np * 4);
-    cudaMemset(m->Vv, 0, m->np * 4);
-    cudaMemset(m->X, 0, (size_t)B * K1 * 2);
-    cudaMemset(m->Xf, 0, (size_t)B * K1 * 4);
-    cudaMemset(m->err, 0, 4);
+    cudaMemsetAsync(m->Mm, 0, m->np * 4, m->s);
+    cudaMemsetAsync(m->Vv, 0, m->np * 4, m->s);
+    cudaMemsetAsync(m->X, 0, (size_t)B * K1 * 2, m->s);
+    cudaMemsetAsync(m->Xf, 0, (size_t)B * K1 * 4, m->s);
+    cudaMemsetAsync(m->err, 0, 4, m->s);
     k_weights_bf16<<<256, 256, 0, m->s>>>(m->W1, m->W1b, nullptr, H, K1);
     k_weights_bf16<<<64, 256, 0, m->s>>>(m->W2, m->W2b, m->W2bT, H, H);
     e = cudaStreamSynchronize(m->s);
@@ -393,15 +393,34 @@ extern "C" int lcmc_mlp_create(int n_in, int hidden, int max_batch, uint64_t see
     return LCMC_OK;
 }
 
-// forward on the first n rows of m->X (padded batch of B rows) -> m->y
-static void mlp_forward(lcmc_mlp *m, int B)
+// forward on the B (multiple of 128) rows of m->X -> activations A2
+static void mlp_forward_s(lcmc_mlp *m, int B, cudaStream_t s)
 {
     const int H = m->hid, K1 = m->k1;
-    gemm_tc(m->X, K1, m->W1b, K1, m->Z1, H, B, H, K1, 0, m->err, m->s);
-    k_bias_act<<<(B * H + 255) / 256, 256, 0, m->s>>>(m->Z1, m->b1, m->H1, m->H1T, nullptr, B, H);
-    gemm_tc(m->H1, H, m->W2b, H, m->Z2, H, B, H, H, 0, m->err, m->s);
-    k_bias_act<<<(B * H + 255) / 256, 256, 0, m->s>>>(m->Z2, m->b2, m->H2, nullptr, m->A2, B, H);
+    gemm_tc(m->X, K1, m->W1b, K1, m->Z1, H, B, H, K1, 0, m->err, s);
+    k_bias_act<<<(B * H + 255) / 256, 256, 0, s>>>(m->Z1, m->b1, m->H1, m->H1T, nullptr, B, H);
+    gemm_tc(m->H1, H, m->W2b, H, m->Z2, H, B, H, H, 0, m->err, s);
+    k_bias_act<<<(B * H + 255) / 256, 256, 0, s>>>(m->Z2, m->b2, m->H2, nullptr, m->A2, B, H);
 }
+static void mlp_forward(lcmc_mlp *m, int B) { mlp_forward_s(m, B, m->s); }
+
+namespace lcmc {
+// In-sweep inference: the sweep's kernels write the BF16 input rows into
+// mlp_input() (leading dimension mlp_ld()), then the forward pass and the
+// output layer run on the sweep's stream; returns the device output vector.
+void *mlp_input(lcmc_mlp *m) { return m->X; }
+int mlp_ld(lcmc_mlp *m) { return m->k1; }
+int mlp_bmax(lcmc_mlp *m) { return m->bmax; }
+int mlp_n_in(lcmc_mlp *m) { return m->n_in; }
+const float *mlp_forward_device(lcmc_mlp *m, int B, cudaStream_t s)
+{
+    mlp_forward_s(m, B, s);
+    k_out_layer<<<(B * 32 + 255) / 256, 256, 0, s>>>(m->A2, m->w3, m->b3, m->y, nullptr, nullptr, nullptr, B, m->hid,
+                                                     B);
+    return m->y;
+}
+int *mlp_err(lcmc_mlp *m) { return m->err; }
+} // namespace lcmc
 
 // rows of host features (n x n_in, FP32) -> m->X (BF16, padded to k1 columns, B rows)
 static void load_batch(lcmc_mlp *m, const float *x, int n, int B)

@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(128) k_energy_exact(DevView v, double *e0, dou
         const int r = v.p2r[i];
         const Replica &p = v.rep[r];
         const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
-        if (scaled && p.ensemble != 2) continue;
+        if (scaled && (p.ensemble != 2 || (p.da_on && !p.vol_stage1))) continue; // NVT, or screened out
         const int cell = v.scid[i] - p.cell_off;
         const int cx = cell % nc0, cy = (cell / nc0) % nc1, cz = cell / (nc0 * nc1);
         int c = -1;

@@ -138,6 +138,47 @@ class GBSystem:
                                                d.ctypes.data_as(_lib.DP)))
         return Q, P2.value, d
 
+    # -- NPT volume moves: learned screen, recordings --
+    def set_surrogate(self, surrogate):
+        """Delayed-acceptance volume moves with a trained da.Surrogate (None: plain)."""
+        if surrogate is None:
+            self._check(lib().lcmc_set_surrogate(self._h, None, 1.0))
+            self._surrogate = None
+        else:
+            self._check(lib().lcmc_set_surrogate(self._h, surrogate.handle, surrogate.scale))
+            self._surrogate = surrogate  # keep it alive while set
+
+    def record_volume_samples(self, capacity):
+        """Record (features, exact dU / N) of the next `capacity` exactly
+        evaluated volume moves (0 stops and frees)."""
+        self._check(lib().lcmc_record_volume_samples(self._h, capacity))
+        self.samples_capacity = capacity
+
+    def get_volume_samples(self):
+        """Recorded samples: features (n, 4097) float32 and dU / N (n,)."""
+        cap = getattr(self, "samples_capacity", 0)
+        x = np.zeros((max(cap, 1), _lib.N_FEATURES), dtype=np.float32)
+        y = np.zeros(max(cap, 1), dtype=np.float32)
+        n = lib().lcmc_get_volume_samples(self._h, x.ctypes.data_as(_lib.FP), y.ctypes.data_as(_lib.FP), cap)
+        if n < 0:
+            self._check(n)
+        return x[:n], y[:n].astype(np.float64)
+
+    def record_history(self, capacity):
+        """Keep a per-sweep row (sweep, Q sums, energy, volume) of the last
+        `capacity` sweeps of every replica (0 stops and frees)."""
+        self._check(lib().lcmc_record_history(self._h, capacity))
+        self.history_capacity = capacity
+
+    def get_history(self, replica=0):
+        """Recorded rows in sweep order, shape (n, 9)."""
+        cap = getattr(self, "history_capacity", 0)
+        rows = np.zeros((max(cap, 1), 9))
+        n = lib().lcmc_get_history(self._h, replica, rows.ctypes.data_as(_lib.DP), cap)
+        if n < 0:
+            self._check(n)
+        return rows[:n]
+
     # -- measurement --
     def stream_handle(self):
         """cudaStream_t of this context (as an integer) for event timing."""
