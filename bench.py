@@ -15,6 +15,11 @@ between sweeps); `e2e` times the public C ABI with host arrays in pinned
 memory: upload + sweep + download every step.  `--impl reference` times the
 reference's own attempt_monte_carlo_move (MCnptColloid.c, built in
 oracle/_ref with its OpenMP pragmas) on the host cores.
+
+The line also carries `npt_da`: effective samples per second of the P2 (and
+volume) series of NPT sweeps at N = 262,144 with a colloid (R = 8), plain
+volume moves against delayed acceptance with the learned surrogate
+(`--da-sweeps` per arm, 0 skips it).
 """
 import argparse
 import ctypes as C
@@ -215,14 +220,144 @@ def kernel_traffic():
 
 
 # ---------------------------------------------------------------------------
+# NPT P2 ESS/s: delayed-acceptance volume moves vs plain
+# ---------------------------------------------------------------------------
+GB_NPT = dict(gb_kappa=3.0, gb_kappa_prime=5.0, gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
+              max_displacement=0.1, max_rotation=0.1)
+
+
+def dilute_start(n, rho0, R, seed):
+    """Simple-cubic start at density rho0 with uniform orientations, no site
+    within R + 2.5 of the colloid centre.  At rho0 = 0.06 the spacing (2.4)
+    leaves no pair inside the reference's flat 1e9 overlap clamp (distreal <
+    0.001) and no rod inside the colloid's 1e8 clamp; a lattice at rho = 0.3
+    with random orientations does, and such rods never leave the clamp."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    L = (n / rho0 + 4.0 * np.pi * R ** 3 / 3.0) ** (1.0 / 3.0)
+    ns = int(np.ceil((1.3 * n) ** (1.0 / 3.0)))
+    while True:
+        g = (np.arange(ns) + 0.5) * (L / ns)
+        X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+        pos = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+        ok = np.linalg.norm(pos - 0.5 * L, axis=1) > R + 2.5
+        if ok.sum() >= n:
+            break
+        ns += 1
+    pos = pos[ok][rng.permutation(int(ok.sum()))[:n]]
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    return [np.ascontiguousarray(a) for a in (pos[:, 0], pos[:, 1], pos[:, 2], u[:, 0], u[:, 1], u[:, 2])], \
+        np.array([L, L, L])
+
+
+def npt_params(lcmc, n, T, P, R, seed, dlnv):
+    return lcmc.default_params(num_particles=n, system_density=0.06, system_temperature=T, system_pressure=P,
+                               mc_ensemble_type=2, npt_max_dlnV=dlnv, colloid_wall_option=1, colloid_radius=R,
+                               rng_seed=seed, precision_mode=1, cell_capacity=64, **GB_NPT)
+
+
+def timed_sweeps(torch, s, k):
+    ext = torch.cuda.ExternalStream(s.stream_handle())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(ext)
+    s.sweep(k)
+    b.record(ext)
+    b.synchronize()
+    return a.elapsed_time(b) * 1e-3
+
+
+def npt_da(lcmc, torch, sweeps, train_sweeps):
+    """P2 (and volume) effective samples per second of NPT sweeps at N = 262,144
+    with a colloid of R = 8 (T* = 0.85, P* = 2, dlnV_max = 0.01), plain volume
+    moves vs delayed acceptance with the surrogate trained on N = 32,768
+    systems (R = 5, T* = 0.9)."""
+    import numpy as np
+
+    from parellel_mc_mpi_for_liquidcrystalsystems_b200 import da
+    t_start = time.perf_counter()
+    # training samples: 16 replicas, compressed from dilute starts, pressures 2..4
+    nr, n1 = 16, 32768
+    pres = [2.0 + 2.0 * r / (nr - 1) for r in range(nr)]
+    with lcmc.GBSystem([npt_params(lcmc, n1, 0.9, pres[r], 5.0, 200 + r, 0.05) for r in range(nr)]) as s:
+        for r in range(nr):
+            st, box = dilute_start(n1, 0.06, 5.0, 300 + r)
+            s.upload(*st, box, replica=r)
+        s.sweep(600)
+        states = [s.download(r) for r in range(nr)]
+    with lcmc.GBSystem([npt_params(lcmc, n1, 0.9, pres[r], 5.0, 400 + r, 0.01) for r in range(nr)]) as s:
+        for r in range(nr):
+            s.upload(*states[r][0], states[r][1], replica=r)
+        s.sweep(100)
+        x, y = da.collect_samples(s, train_sweeps)
+        rho = [n1 / np.prod(s.stats(r)["box"]) for r in range(nr)]
+    sur = da.Surrogate(max_batch=512, seed=1)
+    t0 = time.perf_counter()
+    sur.fit(x, y, epochs=20, batch=256, lr=1e-3)
+    t_train = time.perf_counter() - t0
+    keep = np.abs(y) < 1000.0
+    k = min(4000, int(keep.sum()))
+    corr = float(np.corrcoef(sur.predict(x[keep][:k]), y[keep][:k])[0, 1])
+
+    # the N = 262,144 system: compress from a dilute start, then both arms from one state
+    n = 262144
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05)) as s:
+        st, box = dilute_start(n, 0.06, 8.0, 12)
+        s.upload(*st, box)
+        s.sweep(1000)
+        st4, box4 = s.download()
+    arms = {}
+    for name, use in (("plain", False), ("delayed", True)):
+        with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01)) as s:
+            s.upload(*st4, box4)
+            s.set_surrogate(sur if use else None)
+            s.sweep(300)
+            st0 = s.stats()
+            s.record_history(sweeps)
+            secs = timed_sweeps(torch, s, sweeps)
+            st1 = s.stats()
+            _, p2, E, V = da.p2_series(s)
+            tp, tv = da.integrated_autocorrelation_time(p2), da.integrated_autocorrelation_time(V)
+            arms[name] = {
+                "sweeps": sweeps, "seconds": secs, "ms_per_sweep": 1e3 * secs / sweeps,
+                "p2_mean": float(p2.mean()), "p2_tau_sweeps": tp, "p2_ess": sweeps / (2 * tp),
+                "p2_ess_per_s": sweeps / (2 * tp) / secs, "volume_tau_sweeps": tv,
+                "volume_ess_per_s": sweeps / (2 * tv) / secs, "rho_mean": float(np.mean(n / V)),
+                "volume_accepted": st1["volume_accepted"] - st0["volume_accepted"],
+                "volume_stage1_rejected": st1["volume_stage1_rejected"] - st0["volume_stage1_rejected"],
+                "sweep_ms_parts": [round(float(t), 4) for t in s.last_sweep_timing()]}
+    sur.close()
+    pl, de = arms["plain"], arms["delayed"]
+    return {
+        "metric": "NPT P2 ESS/s, delayed-accept vs plain",
+        "workload": "NPT N=262144, colloid R=8, T*=0.85, P*=2.0, dlnV_max=0.01 (one move per sweep), GB(3,5,2,1), "
+                    "FP32 sweeps, FP64 volume energies; compressed for 1000 sweeps (dlnV_max 0.05) from a dilute "
+                    "lattice (rho 0.06), then 300 sweeps before each timed arm",
+        "training": {"samples": int(len(y)), "used": int(keep.sum()), "replicas": nr, "n": n1, "colloid_R": 5.0,
+                     "T": 0.9, "pressures": [pres[0], pres[-1]], "rho_range": [float(min(rho)), float(max(rho))],
+                     "train_seconds": t_train, "final_loss": sur.history[-1] if sur.history else None,
+                     "pred_corr": corr},
+        "plain": pl, "delayed": de,
+        "p2_ess_per_s_ratio": de["p2_ess_per_s"] / pl["p2_ess_per_s"],
+        "volume_ess_per_s_ratio": de["volume_ess_per_s"] / pl["volume_ess_per_s"],
+        "sweeps_per_s_ratio": pl["ms_per_sweep"] / de["ms_per_sweep"],
+        "ess_note": "tau_int by Sokal's automatic window (c=5); with tau of a few hundred sweeps the ESS of one "
+                    "arm has a relative error of tens of percent",
+        "seconds_total": time.perf_counter() - t_start}
+
+
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--da-sweeps", type=int, default=4000,
+                    help="sweeps per arm of the NPT delayed-acceptance measurement (0 skips it)")
+    ap.add_argument("--da-train-sweeps", type=int, default=400)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -239,7 +374,8 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
                 "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * N_PART / res["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded lattice)", "config": dict(WORKLOAD, parallelism="cpu openmp"),
+                "data": "synthetic (seeded lattice)",
+                "config": dict(WORKLOAD, parallelism="cpu openmp", precision="fp64 (the reference's own code)"),
                 "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -303,22 +439,22 @@ def main():
     flop_launch = flop_att * N_PART / launches_phase
     achieved = flop_launch / (avg_launch_ms * 1e-3) / 1e12
 
-    # e2e through the C ABI: pinned host arrays, upload + sweep + download every step
-    state, box = s.download()
+    # e2e through the C ABI: the caller's state in pinned host arrays; every
+    # step uploads it with the caller's running energy (the in/out energy of
+    # attempt_monte_carlo_move), sweeps, downloads it and reads the energy back
     pinned = [torch.empty(N_PART, dtype=torch.float64, pin_memory=True) for _ in range(6)]
     hv = [p.numpy() for p in pinned]
-    for h, x in zip(hv, state):
-        h[:] = x
+    _, box = s.download(out=hv)
+    energy = s.stats()["energy"]
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        s.upload(*hv, box)
+        s.upload(*hv, box, energy=energy)
         s.sweep(1)
-        out, box = s.download()
-        for h, x in zip(hv, out):
-            h[:] = x
+        _, box = s.download(out=hv)
+        energy = s.stats()["energy"]
     e2e_s = time.perf_counter() - t0
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
@@ -340,14 +476,19 @@ def main():
     cpu, why = reference_cpu(N_PART, seconds=args.cpu_seconds) if world == 1 else (None, "rank 0 of N>1")
     clocks = clk.summary()
     traffic = kernel_traffic()
+    npt = None
+    if args.da_sweeps > 0 and world == 1:
+        npt = npt_da(lcmc, torch, args.da_sweeps, args.da_train_sweeps)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded lattice, relaxing from the lattice start)",
         "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single system",
                        l2="flushed between sweeps (256 MiB memset)"),
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * N_PART + 4 * N_PART + 24,
-                "d2h_bytes_per_step": 6 * 8 * N_PART + 24},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * N_PART + 24 + 8,
+                "d2h_bytes_per_step": 6 * 8 * N_PART + 24 + 8,
+                "step": "lcmc_upload_with_energy (pinned host SoA, caller-carried energy) + lcmc_sweep + "
+                        "lcmc_download (into the pinned arrays) + lcmc_get_stats"},
         "gpu_launches": kps * args.steps,
         "roofline": {"bound": "fp32", "kernel": "k_phase_fast", "achieved": achieved, "peak": sgemm,
                      "unit": "TFLOP/s", "frac": achieved / sgemm,
@@ -364,6 +505,8 @@ def main():
         line["clocks"] = clocks
     if peaks:
         line["measured_peaks"] = {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")}
+    if npt:
+        line["npt_da"] = npt
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

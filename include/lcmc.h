@@ -141,9 +141,19 @@ int lcmc_lattice(const lcmc_params *p, int replica, double *px, double *py, doub
                  double *oz, double box[3]);
 
 /* Copy the caller's SoA arrays (positions in [0, L], orientations) to the
- * device and recompute the total energy in FP64. */
+ * device and recompute the total energy in FP64.  The arrays are checked on
+ * the device (box bounds, no rod centre inside the colloid as in
+ * check_no_colloid_overlaps, MCnptColloid.c:1324-1340, finite non-zero
+ * orientations); a rejected upload leaves the replica's state unchanged. */
 int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz, const double *ox,
                 const double *oy, const double *oz, int n, const double box[3]);
+/* As lcmc_upload, with the caller's running energy in place of the FP64
+ * recompute: the energy in/out argument of attempt_monte_carlo_move
+ * (MCnptColloid.c:2445-2454, `double *system_energy`), whose caller carries
+ * the energy from call to call.  The replica's energy becomes `energy`. */
+int lcmc_upload_with_energy(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz,
+                            const double *ox, const double *oy, const double *oz, int n, const double box[3],
+                            double energy);
 int lcmc_download(lcmc_ctx *ctx, int replica, double *px, double *py, double *pz, double *ox, double *oy, double *oz,
                   int n, double box[3]);
 
@@ -208,17 +218,18 @@ int lcmc_mlp_set_params(lcmc_mlp *m, const float *params);
 int lcmc_gemm_bf16(const float *A, const float *B, float *C, int M, int N, int K);
 
 /* Delayed-acceptance volume moves (Christen & Fox 2005) for the NPT replicas of
- * a context: stage 1 tests the surrogate's antisymmetric energy change
- *   dU~ = N s [g(phi(x), delta) - g(phi(y), -delta)] / 2
+ * a context: stage 1 tests the surrogate's energy change
+ *   dU~ = N s delta [g(phi(x), |delta|) + g(phi(y), |delta|)] / 2
  * (features phi: density, Q tensor and radial alignment on an 8^3 grid, 4097
- * inputs with delta ln V), and only moves that pass it get the exact FP64
- * recompute and stage 2, exp(-beta (dU - dU~)).  s = target_scale converts the
- * network output to dU / N.  m = NULL switches it off.  The network must stay
+ * inputs with |delta ln V|; g predicts the slope dU / (N delta)), which is odd
+ * under x <-> y, and only moves that pass it get the exact FP64 recompute and
+ * stage 2, exp(-beta (dU - dU~)).  s = target_scale converts the network
+ * output to dU / (N delta).  m = NULL switches it off.  The network must stay
  * alive while set. */
 int lcmc_set_surrogate(lcmc_ctx *ctx, lcmc_mlp *m, double target_scale);
 #define LCMC_FEATURES 4097
-/* Record (features of x, exact dU / N) of every exactly evaluated volume move
- * (capacity samples; 0 stops and frees); fetch them (x: n x 4097). */
+/* Record (features of x, exact dU / (N delta)) of every exactly evaluated
+ * volume move (capacity samples; 0 stops and frees); fetch them (x: n x 4097). */
 int lcmc_record_volume_samples(lcmc_ctx *ctx, int capacity);
 int lcmc_get_volume_samples(lcmc_ctx *ctx, float *x, float *y, int max_n);
 /* Per-sweep history (last `capacity` sweeps): rows of 9 doubles = sweep,

@@ -67,6 +67,7 @@ EXPORTS = {
     "lcmc_init_config": ([C.c_void_p, C.c_int], C.c_int),
     "lcmc_lattice": ([C.POINTER(Params), C.c_int, DP, DP, DP, DP, DP, DP, DP], C.c_int),
     "lcmc_upload": ([C.c_void_p, C.c_int, DP, DP, DP, DP, DP, DP, C.c_int, DP], C.c_int),
+    "lcmc_upload_with_energy": ([C.c_void_p, C.c_int, DP, DP, DP, DP, DP, DP, C.c_int, DP, C.c_double], C.c_int),
     "lcmc_download": ([C.c_void_p, C.c_int, DP, DP, DP, DP, DP, DP, C.c_int, DP], C.c_int),
     "lcmc_sweep": ([C.c_void_p, C.c_int], C.c_int),
     "lcmc_get_stats": ([C.c_void_p, C.c_int, C.POINTER(Stats)], C.c_int),

@@ -12,6 +12,7 @@
 
 #include <string>
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "../../include/lcmc.h"
@@ -37,7 +38,7 @@ struct lcmc_ctx {
     double *d_x[2][6] = {{nullptr}};
     int *d_id[2] = {nullptr, nullptr};
     int *d_cid = nullptr, *d_rank = nullptr, *d_perm = nullptr, *d_scid = nullptr;
-    int *d_cell_count = nullptr, *d_cell_start = nullptr, *d_block_sums = nullptr;
+    int *d_cell_count = nullptr, *d_cell_start = nullptr, *d_block_sums = nullptr, *d_flag = nullptr;
     double *d_cell_e0 = nullptr, *d_cell_e1 = nullptr;
     int *d_cell_n0 = nullptr, *d_cell_n1 = nullptr;
     unsigned long long *d_cell_pairs = nullptr, *d_cell_cands = nullptr;
@@ -45,6 +46,8 @@ struct lcmc_ctx {
     double *d_pe0 = nullptr, *d_pe1 = nullptr;
     int *d_phard = nullptr;
     double *d_red = nullptr;
+    double *d_red_part = nullptr; // chunk partial sums
+    int red_nchunk = 1;
     double *d_trial_d[8] = {nullptr}; // tnx tny tnz tux tuy tuz tdU tlu
     float *d_trial_f[3] = {nullptr};  // tdx tdy tdz
     unsigned char *d_thard = nullptr;
@@ -64,7 +67,7 @@ struct lcmc_ctx {
     // kernels
     int kernel_override = -1;
     int fast_variant = 0;
-    int grid_elem = 0, grid_exact = 0, grid_fast = 0;
+    int grid_elem = 0, grid_exact = 0, grid_fast = 0, grid_energy = 0;
     bool any_fast = false, any_exact = false, any_npt = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -428,6 +431,8 @@ static DevView view(const lcmc_ctx *c, int parity)
     v.cell_cands = c->d_cell_cands;
     v.outcome = c->d_outcome;
     v.scratch_d = c->d_red;
+    v.red_part = c->d_red_part;
+    v.red_nchunk = c->red_nchunk;
     v.tnx = c->d_trial_d[0];
     v.tny = c->d_trial_d[1];
     v.tnz = c->d_trial_d[2];
@@ -459,9 +464,9 @@ static void free_ctx(lcmc_ctx *c)
     for (int i = 0; i < 5; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     void *ptrs[] = {c->d_rep, c->d_stats, c->d_act_off, c->d_p2r, c->d_id[0], c->d_id[1], c->d_cid, c->d_rank,
-                    c->d_perm, c->d_scid, c->d_cell_count, c->d_cell_start, c->d_block_sums, c->d_cell_e0,
+                    c->d_perm, c->d_scid, c->d_cell_count, c->d_cell_start, c->d_block_sums, c->d_flag, c->d_cell_e0,
                     c->d_cell_e1, c->d_cell_n0, c->d_cell_n1, c->d_cell_pairs, c->d_cell_cands, c->d_outcome,
-                    c->d_pe0, c->d_pe1, c->d_phard, c->d_red};
+                    c->d_pe0, c->d_pe1, c->d_phard, c->d_red, c->d_red_part};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int k = 0; k < 8; k++)
@@ -614,6 +619,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     ALLOC(c->d_cell_count, c->ctot);
     ALLOC(c->d_cell_start, c->ctot + 1);
     ALLOC(c->d_block_sums, 4096);
+    ALLOC(c->d_flag, 1);
     ALLOC(c->d_cell_e0, c->ctot);
     ALLOC(c->d_cell_e1, c->ctot);
     ALLOC(c->d_cell_n0, c->ctot);
@@ -625,6 +631,12 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     ALLOC(c->d_pe1, c->ntot);
     ALLOC(c->d_phard, c->ntot);
     ALLOC(c->d_red, 16 * n + 16);
+    {
+        int nmax = 1;
+        for (int r = 0; r < n; r++) nmax = std::max(nmax, params[r].num_particles);
+        c->red_nchunk = (nmax + LCMC_RED_CHUNK - 1) / LCMC_RED_CHUNK;
+    }
+    ALLOC(c->d_red_part, (size_t)n * c->red_nchunk * 6);
     for (int k = 0; k < 8; k++) ALLOC(c->d_trial_d[k], c->ntot);
     for (int k = 0; k < 3; k++) ALLOC(c->d_trial_f[k], c->ntot);
     ALLOC(c->d_thard, c->ntot);
@@ -649,6 +661,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     choose_kernels(c);
     c->grid_elem = 4 * c->sms;
     c->grid_exact = 4 * c->sms;
+    c->grid_energy = energy_exact_blocks_per_sm() * c->sms;
     c->grid_fast = fast_blocks_per_sm(c->fast_variant) * c->sms;
     int rc = upload_replica_table(c);
     if (rc) {
@@ -724,7 +737,7 @@ static void enqueue_sweep(lcmc_ctx *c, int parity)
             const float *y = mlp_forward_device(c->mlp, B, c->stream);
             launch_da_stage1(v, c->stream, y);
         }
-        launch_volume_finish(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_exact);
+        launch_volume_finish(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_energy);
     }
     cudaEventRecordWithFlags(c->ev[3], c->stream, cudaEventRecordExternal);
     launch_finalize(v, c->stream);
@@ -830,13 +843,14 @@ extern "C" int lcmc_get_stream(lcmc_ctx *ctx, void **stream)
 extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
 {
     if (!ctx) return LCMC_EINVAL;
-    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases; volume: propose, energy, accept, scale;
-    // surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1; recording; history; finalize
-    int n = 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 4 * (int)ctx->any_npt + 1;
+    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases; volume: propose, energy, chunk sums, accept,
+    // scale; surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1; recording; history: chunk sums,
+    // rows; finalize
+    int n = 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 1;
     if (ctx->any_npt && (ctx->any_da || ctx->rec_cap > 0)) n += 2;
     if (ctx->any_npt && ctx->any_da) n += 6;
     if (ctx->any_npt && ctx->rec_cap > 0) n += 1;
-    if (ctx->hist_cap > 0) n += 1;
+    if (ctx->hist_cap > 0) n += 2;
     return n;
 }
 
@@ -961,7 +975,7 @@ static int recompute_energy(lcmc_ctx *c, int replica_only)
     enqueue_rebin(c, c->cur);
     c->cur ^= 1;
     DevView v = view(c, c->cur);
-    launch_energy_exact(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, 0, c->grid_exact);
+    launch_energy_exact(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, 0, c->grid_energy);
     launch_energy_reduce(v, c->stream, c->d_pe0, replica_only);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     CUDA_TRY(c, cudaGetLastError());
@@ -978,8 +992,11 @@ extern "C" int lcmc_total_energy(lcmc_ctx *ctx, int replica, int precision, doub
     return LCMC_OK;
 }
 
-extern "C" int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz,
-                           const double *ox, const double *oy, const double *oz, int n, const double box[3])
+// Stage the caller's arrays in the rebin's spare buffer, check them on the
+// device, and only then copy them over the replica's current slots: a rejected
+// upload leaves the context's state as it was.
+static int upload_state(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz,
+                        const double *ox, const double *oy, const double *oz, int n, const double box[3])
 {
     if (!ctx || replica < 0 || replica >= ctx->R || !px || !py || !pz || !ox || !oy || !oz || !box)
         return LCMC_EINVAL;
@@ -988,32 +1005,42 @@ extern "C" int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const d
     const double rc = ctx->params[replica].cutoff_radius;
     for (int a = 0; a < 3; a++)
         if (!(box[a] >= 2.0 * rc)) return set_err(ctx, LCMC_EBOX, "box shorter than twice the cutoff");
-    // check_no_colloid_overlaps (MCnptColloid.c:1324-1340) and the box bounds
     const double R = ctx->params[replica].colloid_radius;
-    for (int i = 0; i < n; i++) {
-        if (!(px[i] >= 0.0 && px[i] <= box[0] && py[i] >= 0.0 && py[i] <= box[1] && pz[i] >= 0.0 && pz[i] <= box[2]))
-            return set_err(ctx, LCMC_EINVAL, "particle outside the box");
-        double dx = px[i] - 0.5 * box[0], dy = py[i] - 0.5 * box[1], dz = pz[i] - 0.5 * box[2];
-        if (dx * dx + dy * dy + dz * dz < R * R) return set_err(ctx, LCMC_EOVERLAP, "particle inside the colloid");
-        double n2 = ox[i] * ox[i] + oy[i] * oy[i] + oz[i] * oz[i];
-        if (!(n2 > 0.0) || !(n2 < 1e300)) return set_err(ctx, LCMC_EINVAL, "zero or non-finite orientation");
-    }
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    const int off = rp.p_off;
+    const int off = rp.p_off, cur = ctx->cur, spare = cur ^ 1;
     const double *src[6] = {px, py, pz, ox, oy, oz};
-    for (int k = 0; k < 6; k++)
-        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_x[ctx->cur][k] + off, src[k], sizeof(double) * n, cudaMemcpyHostToDevice,
+    const double *stage[6];
+    for (int k = 0; k < 6; k++) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_x[spare][k] + off, src[k], sizeof(double) * n, cudaMemcpyHostToDevice,
                                       ctx->stream));
-    std::vector<int> ids(n);
-    for (int i = 0; i < n; i++) ids[i] = i;
-    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_id[ctx->cur] + off, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice,
-                                  ctx->stream));
+        stage[k] = ctx->d_x[spare][k] + off;
+    }
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    launch_validate_upload(stage, ctx->d_id[spare] + off, n, box, R * R, ctx->d_flag, ctx->stream, ctx->grid_elem);
+    int flag = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (flag & 1) return set_err(ctx, LCMC_EINVAL, "particle outside the box");
+    if (flag & 2) return set_err(ctx, LCMC_EOVERLAP, "particle inside the colloid");
+    if (flag & 4) return set_err(ctx, LCMC_EINVAL, "zero or non-finite orientation");
+    for (int k = 0; k < 6; k++)
+        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_x[cur][k] + off, stage[k], sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_id[cur] + off, ctx->d_id[spare] + off, sizeof(int) * n,
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
     for (int a = 0; a < 3; a++) rp.L[a] = box[a];
     // box (dynamic field) into the device table
     CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * replica + offsetof(Replica, L), rp.L,
                                   sizeof(double) * 3, cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->uploaded[replica] = 1;
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz,
+                           const double *ox, const double *oy, const double *oz, int n, const double box[3])
+{
+    int rc = upload_state(ctx, replica, px, py, pz, ox, oy, oz, n, box);
+    if (rc) return rc;
     bool all = true;
     for (int r = 0; r < ctx->R; r++) all = all && ctx->uploaded[r];
     if (!all) return LCMC_OK; // energies are computed once every replica holds a configuration
@@ -1024,6 +1051,25 @@ extern "C" int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const d
     CUDA_TRY(ctx, cudaMemcpy(st.data(), ctx->d_stats, sizeof(DevStats) * ctx->R, cudaMemcpyDeviceToHost));
     for (auto &s : st) s.drift = 0.0;
     CUDA_TRY(ctx, cudaMemcpy(ctx->d_stats, st.data(), sizeof(DevStats) * ctx->R, cudaMemcpyHostToDevice));
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_upload_with_energy(lcmc_ctx *ctx, int replica, const double *px, const double *py,
+                                       const double *pz, const double *ox, const double *oy, const double *oz, int n,
+                                       const double box[3], double energy)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R) return LCMC_EINVAL;
+    if (!std::isfinite(energy)) return set_err(ctx, LCMC_EINVAL, "non-finite energy");
+    int rc = upload_state(ctx, replica, px, py, pz, ox, oy, oz, n, box);
+    if (rc) return rc;
+    // the caller's running energy replaces the recompute (no drift recorded)
+    const size_t base = sizeof(DevStats) * replica;
+    const double zero = 0.0;
+    CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_stats + base + offsetof(DevStats, energy), &energy, sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_stats + base + offsetof(DevStats, drift), &zero, sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return LCMC_OK;
 }
 

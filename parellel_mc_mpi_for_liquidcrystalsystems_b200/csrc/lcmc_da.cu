@@ -3,25 +3,32 @@
 // the reference has no NPT move, MCnptColloid.c:3978).
 //
 // Features of a configuration x (8 channels on an 8^3 grid of the box in
-// fractional coordinates, channel-major, then the move's delta ln V):
-//   0  number density / 0.3          (scales by V/V' = e^-delta under the move)
+// fractional coordinates, channel-major, then the move's |delta ln V|):
+//   0  number density / 0.3
 //   1-5 Q tensor: <ux ux> - 1/3, <ux uy>, <ux uz>, <uy uy> - 1/3, <uy uz>
 //   6  radial alignment <(u . r_hat)^2> - 1/3, r_hat from the colloid centre
-//   7  (density / 0.3)^2                 (scales by e^-2 delta)
-//   4096: delta / delta_max
-// Under the affine volume move every channel of the scaled configuration y
-// follows from x analytically, so the surrogate
-//   dU~(x -> y) = N s [g(phi(x), delta) - g(phi(y), -delta)] / 2
-// is antisymmetric, dU~(y -> x) = -dU~(x -> y), and the two-stage test
-// (Christen & Fox, J. Comput. Graph. Stat. 14 (2005) 795) keeps detailed
-// balance:
+//   7  (density / 0.3)^2
+//   4096: |delta| / delta_max
+// The network g predicts the slope dU / (N delta) of a move of size |delta|.
+// The surrogate energy change is
+//   dU~(x -> y) = N s delta [g(phi(x), |delta|) + g(phi(y), |delta|)] / 2,
+// symmetric in its two evaluations and odd in delta, so dU~(y -> x) =
+// -dU~(x -> y) exactly and the two-stage test (Christen & Fox, J. Comput.
+// Graph. Stat. 14 (2005) 795) keeps detailed balance:
 //   stage 1: ln A1 = -beta (dU~ + P dV) + (N + 1) delta
 //   stage 2 (exact FP64 dU, only after stage 1 passed): ln A2 = -beta (dU - dU~)
+// Under the affine volume move the features of the scaled configuration y
+// follow from those of x (cells, orientations and radial directions are
+// unchanged; only the density channels see the new volume), so both rows are
+// built from one pass over x.  The two network rows are averaged, not
+// differenced: a difference of two nearly equal BF16-input outputs would be
+// mostly rounding.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "lcmc_internal.h"
 #include "lcmc_launch.h"
+#include "lcmc_reduce.cuh"
 #include "lcmc_rng.cuh"
 
 namespace lcmc {
@@ -71,8 +78,8 @@ __global__ void k_feat_accum(DevView v)
 
 __device__ __forceinline__ double from_fixed(unsigned long long a) { return (double)(long long)a / FIX_ONE; }
 
-// rows 2r (x, +delta) and 2r + 1 (y, -delta) of the surrogate's BF16 input;
-// the x row also in FP32 (feat_f) for sample recording.
+// rows 2r (x) and 2r + 1 (y), both with |delta|, of the surrogate's BF16
+// input; the x row also in FP32 (feat_f) for sample recording.
 __global__ void k_feat_finalize(DevView v, __nv_bfloat16 *X, int ldx)
 {
     const int r = blockIdx.x;
@@ -87,7 +94,7 @@ __global__ void k_feat_finalize(DevView v, __nv_bfloat16 *X, int ldx)
     const double lam = p.vol_lambda;
     const double Vy = (p.L[0] * lam) * (p.L[1] * lam) * (p.L[2] * lam);
     const double inv_vc_y = (double)FC / Vy / 0.3;
-    const float dn = (float)(p.dlnv_max > 0.0 ? p.vol_delta / p.dlnv_max : 0.0);
+    const float dn = (float)(p.dlnv_max > 0.0 ? fabs(p.vol_delta) / p.dlnv_max : 0.0);
     __nv_bfloat16 *rx = X ? X + (size_t)(2 * r) * ldx : nullptr;
     __nv_bfloat16 *ry = X ? X + (size_t)(2 * r + 1) * ldx : nullptr;
     float *rf = v.feat_f + (size_t)r * LCMC_FEAT;
@@ -119,7 +126,7 @@ __global__ void k_feat_finalize(DevView v, __nv_bfloat16 *X, int ldx)
         rf[8 * FC] = dn;
         if (rx) {
             rx[8 * FC] = __float2bfloat16(dn);
-            ry[8 * FC] = __float2bfloat16(-dn);
+            ry[8 * FC] = __float2bfloat16(dn);
         }
     }
 }
@@ -134,7 +141,7 @@ __global__ void k_da_stage1(DevView v, const float *y)
             p.vol_stage1 = 1;
             continue;
         }
-        const double dUs = (double)p.n * p.da_scale * 0.5 * ((double)y[2 * r] - (double)y[2 * r + 1]);
+        const double dUs = (double)p.n * p.da_scale * p.vol_delta * 0.5 * ((double)y[2 * r] + (double)y[2 * r + 1]);
         const double V = p.L[0] * p.L[1] * p.L[2];
         const double dV = V * expm1_small(p.vol_delta);
         const double lnA1 = -p.k.beta * (dUs + p.pressure * dV) + (double)(p.n + 1) * p.vol_delta;
@@ -144,54 +151,42 @@ __global__ void k_da_stage1(DevView v, const float *y)
     }
 }
 
-// Copy this sweep's (features of x, delta, exact dU / N) of every NPT replica
-// whose exact volume energy was computed into the sample ring.
+// Copy this sweep's (features of x with |delta|, exact slope dU / (N delta))
+// of every NPT replica whose exact volume energy was computed into the sample
+// ring, in replica order (one block, so the ring's order repeats run to run).
+// delta is never 0: it is dlnV_max (2u - 1) with u = (k + 1/2) / 2^32.
 __global__ void k_record_samples(DevView v)
 {
-    const int r = blockIdx.x;
-    const Replica &p = v.rep[r];
-    if (p.ensemble != 2 || v.rec_cap <= 0 || p.vol_state == 3 || !p.vol_stage1) return;
-    __shared__ int slot;
-    if (threadIdx.x == 0) slot = atomicAdd(v.rec_count, 1);
-    __syncthreads();
-    if (slot >= v.rec_cap) return;
-    const float *src = v.feat_f + (size_t)r * LCMC_FEAT;
-    float *dst = v.rec_x + (size_t)slot * LCMC_FEAT;
-    for (int k = threadIdx.x; k < LCMC_FEAT; k += blockDim.x) dst[k] = src[k];
-    if (threadIdx.x == 0) v.rec_y[slot] = (float)((p.vol_U_new - p.vol_U_old) / (double)p.n);
+    if (v.rec_cap <= 0) return;
+    int slot = *v.rec_count;
+    for (int r = 0; r < v.R; r++) {
+        const Replica &p = v.rep[r];
+        if (p.ensemble != 2 || p.vol_state == 3 || !p.vol_stage1) continue;
+        if (slot < v.rec_cap) {
+            const float *src = v.feat_f + (size_t)r * LCMC_FEAT;
+            float *dst = v.rec_x + (size_t)slot * LCMC_FEAT;
+            for (int k = threadIdx.x; k < LCMC_FEAT; k += blockDim.x) dst[k] = src[k];
+            if (threadIdx.x == 0)
+                v.rec_y[slot] = (float)((p.vol_U_new - p.vol_U_old) / ((double)p.n * p.vol_delta));
+        }
+        slot++;
+    }
+    __syncthreads(); // every thread has read the old count
+    if (threadIdx.x == 0) *v.rec_count = slot;
 }
 
 // Per-sweep history of every replica: sweep, Q-tensor sums (6), energy, volume.
-__global__ void k_hist_record(DevView v)
+__global__ void __launch_bounds__(256) k_hist_record(DevView v)
 {
     const int r = blockIdx.x;
     const Replica &p = v.rep[r];
-    __shared__ double sh[256];
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < p.n; i += blockDim.x) {
-        const int g = p.p_off + i;
-        const double x = v.ox[g], y = v.oy[g], z = v.oz[g];
-        s[0] += x * x;
-        s[1] += x * y;
-        s[2] += x * z;
-        s[3] += y * y;
-        s[4] += y * z;
-        s[5] += z * z;
-    }
-    const unsigned long long sw = p.sweep - 1ull; // finalize already counted this sweep
-    double *row = v.hist + ((size_t)r * v.hist_cap + (size_t)(sw % (unsigned long long)v.hist_cap)) * 9;
-    for (int k = 0; k < 6; k++) {
-        sh[threadIdx.x] = s[k];
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) row[1 + k] = sh[0];
-        __syncthreads();
-    }
+    double s[6];
+    finish_sums<6>(v, r, s); // Q-tensor chunk sums, launched just before
     if (threadIdx.x == 0) {
+        const unsigned long long sw = p.sweep - 1ull; // finalize already counted this sweep
+        double *row = v.hist + ((size_t)r * v.hist_cap + (size_t)(sw % (unsigned long long)v.hist_cap)) * 9;
         row[0] = (double)sw;
+        for (int k = 0; k < 6; k++) row[1 + k] = s[k];
         row[7] = v.stats[r].energy;
         row[8] = p.L[0] * p.L[1] * p.L[2];
     }
@@ -205,7 +200,11 @@ void launch_features(const DevView &v, cudaStream_t s, void *X, int ldx, int gri
 }
 
 void launch_da_stage1(const DevView &v, cudaStream_t s, const float *y) { k_da_stage1<<<1, 256, 0, s>>>(v, y); }
-void launch_record_samples(const DevView &v, cudaStream_t s) { k_record_samples<<<v.R, 256, 0, s>>>(v); }
-void launch_hist_record(const DevView &v, cudaStream_t s) { k_hist_record<<<v.R, 256, 0, s>>>(v); }
+void launch_record_samples(const DevView &v, cudaStream_t s) { k_record_samples<<<1, 256, 0, s>>>(v); }
+void launch_hist_record(const DevView &v, cudaStream_t s)
+{
+    launch_q_chunk_sums(v, s);
+    k_hist_record<<<v.R, 256, 0, s>>>(v);
+}
 
 } // namespace lcmc

@@ -59,6 +59,9 @@ struct DevStats {
 constexpr int F_CELLCAP = 1, F_STENCILCAP = 2, F_LISTCAP = 4, F_NONFINITE = 8, F_GRIDCAP = 16;
 
 // Launch view of the device buffers, passed by value to every kernel.
+// particles per chunk of the two-level reductions (sums over a replica)
+constexpr int LCMC_RED_CHUNK = 4096;
+
 struct DevView {
     int R;              // replicas
     int ntot;           // particles, all replicas
@@ -85,6 +88,8 @@ struct DevView {
     unsigned long long *cell_pairs, *cell_cands;
     unsigned char *outcome;    // [ntot] by particle slot of id: 0/1/2
     double *scratch_d;         // [R * 8] small reductions
+    double *red_part;          // [R x red_nchunk x 6] per-chunk partial sums
+    int red_nchunk;            // chunks of LCMC_RED_CHUNK particles per replica (largest replica)
     // this sweep's trial moves, by sorted slot (FP32 kernel systems)
     double *tnx, *tny, *tnz;   // new position, wrapped
     double *tux, *tuy, *tuz;   // new orientation, normalised

@@ -13,6 +13,7 @@ void launch_finalize(const DevView &v, cudaStream_t s);
 // lcmc_sweep_exact.cu (FP64, bit-identical to the CPU oracle)
 void launch_phase_exact(const DevView &v, cudaStream_t s, int ci, int grid);
 void launch_energy_exact(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int scaled, int grid);
+int energy_exact_blocks_per_sm(); // resident blocks of 128 threads per SM
 
 // lcmc_sweep_fast.cu (FP32)
 struct FastVariant {
@@ -24,10 +25,13 @@ void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, in
 int fast_blocks_per_sm(int variant);
 
 // lcmc_misc.cu
+void launch_q_chunk_sums(const DevView &v, cudaStream_t s); // Q-tensor chunk sums of every replica
 void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, int replica_only);
 void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid);
 void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out);
 void launch_to_id_order(const DevView &v, cudaStream_t s, int r, int grid);
+void launch_validate_upload(const double *const x[6], int *id, int n, const double L[3], double R2, int *flag,
+                            cudaStream_t s, int grid);
 
 } // namespace lcmc
 struct lcmc_mlp;

@@ -3,37 +3,68 @@
 #include <cuda_runtime.h>
 
 #include "lcmc_internal.h"
+#include "lcmc_reduce.cuh"
 #include "lcmc_rng.cuh"
 
 namespace lcmc {
 
-// Block-wide sum in a fixed order (thread-strided partials, then a tree).
-template <typename T>
-__device__ __forceinline__ T block_sum(T x, T *sh)
+// Two-level sums over a replica's particles, in a fixed order (results repeat
+// bit for bit): blocks (chunk c, replica r) add LCMC_RED_CHUNK particles each
+// into red_part[(r * red_nchunk + c) * 6 + k], then one block per replica adds
+// its chunks.  One block streaming a whole replica was limited to one SM's
+// bandwidth (1.9 ms for 8 MB at N = 2^20).
+//   mode 0: k = 0 sum of e0 (total energy)
+//   mode 1: k = 0, 1, 2 sums of e0, e1 and hard-core hits (NPT replicas whose
+//           volume move was not screened out)
+//   mode 2: k = 0..5 Q-tensor sums u_x u_x, u_x u_y, u_x u_z, u_y u_y, u_y u_z,
+//           u_z u_z (compute_liquid_crystal_order_parameters,
+//           MCnptColloid.c:2149-2167, in FP64)
+template <int K, int MODE>
+__global__ void __launch_bounds__(256) k_chunk_sums(DevView v, const double *e0, const double *e1, const int *hard)
 {
-    sh[threadIdx.x] = x;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-        __syncthreads();
+    const int c = blockIdx.x, r = blockIdx.y;
+    const Replica &p = v.rep[r];
+    const int i0 = c * LCMC_RED_CHUNK;
+    if (i0 >= p.n) return;
+    if (MODE == 1 && (p.ensemble != 2 || (p.da_on && !p.vol_stage1))) return;
+    const int i1 = min(p.n, i0 + LCMC_RED_CHUNK);
+    double s[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) s[k] = 0.0;
+    for (int i = i0 + (int)threadIdx.x; i < i1; i += blockDim.x) {
+        const int g = p.p_off + i;
+        if (MODE == 0) {
+            s[0] += e0[g];
+        } else if (MODE == 1) {
+            s[0] += e0[g];
+            s[1] += e1[g];
+            s[2] += hard[g] ? 1.0 : 0.0;
+        } else {
+            const double x = v.ox[g], y = v.oy[g], z = v.oz[g];
+            s[0] += x * x;
+            s[1] += x * y;
+            s[2] += x * z;
+            s[3] += y * y;
+            s[4] += y * z;
+            s[5] += z * z;
+        }
     }
-    T r = sh[0];
-    __syncthreads();
-    return r;
+    __shared__ double sh[K][8];
+    block_sums<K>(s, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < K; k++) v.red_part[((size_t)r * v.red_nchunk + c) * 6 + k] = s[k];
 }
 
-// Block per replica: total energy = sum of per-particle energies (deterministic).
-// Resets the running energy to the recomputed value and records the drift.
-__global__ void k_energy_reduce(DevView v, const double *e0, int replica_only)
+// Block per replica: total energy from the chunk sums.  Resets the running
+// energy to the recomputed value and records the drift.
+__global__ void __launch_bounds__(256) k_energy_reduce(DevView v, int replica_only)
 {
     const int r = blockIdx.x;
     if (replica_only >= 0 && r != replica_only) return;
-    const Replica &p = v.rep[r];
-    __shared__ double sh[256];
-    double s = 0.0;
-    for (int i = threadIdx.x; i < p.n; i += blockDim.x) s += e0[p.p_off + i];
-    double tot = block_sum(s, sh);
+    double s[1];
+    finish_sums<1>(v, r, s);
     if (threadIdx.x == 0) {
+        const double tot = s[0];
         DevStats &st = v.stats[r];
         st.drift = st.energy - tot;
         st.energy = tot;
@@ -60,10 +91,10 @@ __global__ void k_volume_propose(DevView v)
     }
 }
 
-// NPT: block per replica.  Sums U(V), U(V') and hard-core hits, then the
-// Metropolis test of the ln V walk:
+// NPT: block per replica.  U(V), U(V') and hard-core hits from the chunk sums,
+// then the Metropolis test of the ln V walk:
 //   ln A = -beta (dU + P dV) + (N + 1) delta,  dV = V (e^delta - 1).
-__global__ void k_volume_accept(DevView v, const double *e0, const double *e1, const int *hard)
+__global__ void __launch_bounds__(256) k_volume_accept(DevView v)
 {
     const int r = blockIdx.x;
     Replica &p = v.rep[r];
@@ -76,19 +107,11 @@ __global__ void k_volume_accept(DevView v, const double *e0, const double *e1, c
         }
         return;
     }
-    __shared__ double sh[256];
-    __shared__ int shi[256];
-    double a = 0.0, b = 0.0;
-    int h = 0;
-    for (int i = threadIdx.x; i < p.n; i += blockDim.x) {
-        a += e0[p.p_off + i];
-        b += e1[p.p_off + i];
-        h |= hard[p.p_off + i];
-    }
-    double U0 = block_sum(a, sh);
-    double U1 = block_sum(b, sh);
-    int H = block_sum(h, shi);
+    double su[3];
+    finish_sums<3>(v, r, su);
     if (threadIdx.x == 0) {
+        const double U0 = su[0], U1 = su[1];
+        const bool H = su[2] > 0.0;
         DevStats &st = v.stats[r];
         st.drift = st.energy - U0;
         st.last_recompute = U0;
@@ -132,28 +155,35 @@ __global__ void k_volume_scale(DevView v)
     }
 }
 
-// Q-tensor sums of one replica: out[0..5] = sum u_x u_x, u_x u_y, u_x u_z,
-// u_y u_y, u_y u_z, u_z u_z (compute_liquid_crystal_order_parameters,
-// MCnptColloid.c:2149-2167, in FP64).
-__global__ void k_order_sums(DevView v, int r, double *out)
+// Q-tensor sums of one replica from the chunk sums (mode 2): out[0..5].
+__global__ void __launch_bounds__(256) k_order_finish(DevView v, int r, double *out)
 {
-    const Replica &p = v.rep[r];
-    __shared__ double sh[256];
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < p.n; i += blockDim.x) {
-        const int g = p.p_off + i;
-        const double x = v.ox[g], y = v.oy[g], z = v.oz[g];
-        s[0] += x * x;
-        s[1] += x * y;
-        s[2] += x * z;
-        s[3] += y * y;
-        s[4] += y * z;
-        s[5] += z * z;
+    double s[6];
+    finish_sums<6>(v, r, s);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 6; k++) out[k] = s[k];
+}
+
+// Checks of an uploaded configuration (check_no_colloid_overlaps,
+// MCnptColloid.c:1324-1340, and the box bounds) on the staged arrays; writes
+// the identity id map.  flag bits: 1 outside the box, 2 inside the colloid,
+// 4 zero or non-finite orientation.
+__global__ void k_validate_upload(const double *px, const double *py, const double *pz, const double *ox,
+                                  const double *oy, const double *oz, int *id, int n, double L0, double L1, double L2,
+                                  double R2, int *flag)
+{
+    int bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double x = px[i], y = py[i], z = pz[i];
+        if (!(x >= 0.0 && x <= L0 && y >= 0.0 && y <= L1 && z >= 0.0 && z <= L2)) bad |= 1;
+        const double dx = x - 0.5 * L0, dy = y - 0.5 * L1, dz = z - 0.5 * L2;
+        if (dx * dx + dy * dy + dz * dz < R2) bad |= 2;
+        const double n2 = ox[i] * ox[i] + oy[i] * oy[i] + oz[i] * oz[i];
+        if (!(n2 > 0.0) || !(n2 < 1e300)) bad |= 4;
+        id[i] = i;
     }
-    for (int k = 0; k < 6; k++) {
-        double t = block_sum(s[k], sh);
-        if (threadIdx.x == 0) out[k] = t;
-    }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (bad && (threadIdx.x & 31) == 0) atomicOr(flag, bad);
 }
 
 // Copy one replica's sorted slots into id order (download) in the q* buffer.
@@ -178,9 +208,17 @@ __global__ void k_to_id_order(DevView v, int r)
 
 namespace lcmc {
 
+static dim3 chunk_grid(const DevView &v) { return dim3(v.red_nchunk, v.R); }
+
 void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, int replica_only)
 {
-    k_energy_reduce<<<v.R, 256, 0, s>>>(v, e0, replica_only);
+    k_chunk_sums<1, 0><<<chunk_grid(v), 256, 0, s>>>(v, e0, nullptr, nullptr);
+    k_energy_reduce<<<v.R, 256, 0, s>>>(v, replica_only);
+}
+
+void launch_q_chunk_sums(const DevView &v, cudaStream_t s)
+{
+    k_chunk_sums<6, 2><<<chunk_grid(v), 256, 0, s>>>(v, nullptr, nullptr, nullptr);
 }
 
 void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid)
@@ -197,12 +235,23 @@ void launch_volume_propose(const DevView &v, cudaStream_t s) { k_volume_propose<
 void launch_volume_finish(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid)
 {
     launch_energy_exact(v, s, e0, e1, hard, 1, grid);
-    k_volume_accept<<<v.R, 256, 0, s>>>(v, e0, e1, hard);
+    k_chunk_sums<3, 1><<<chunk_grid(v), 256, 0, s>>>(v, e0, e1, hard);
+    k_volume_accept<<<v.R, 256, 0, s>>>(v);
     if (v.rec_cap > 0) launch_record_samples(v, s);
     k_volume_scale<<<grid, 256, 0, s>>>(v);
 }
 
-void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out) { k_order_sums<<<1, 256, 0, s>>>(v, r, out); }
+void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out)
+{
+    launch_q_chunk_sums(v, s);
+    k_order_finish<<<1, 256, 0, s>>>(v, r, out);
+}
+
+void launch_validate_upload(const double *const x[6], int *id, int n, const double L[3], double R2, int *flag,
+                            cudaStream_t s, int grid)
+{
+    k_validate_upload<<<grid, 256, 0, s>>>(x[0], x[1], x[2], x[3], x[4], x[5], id, n, L[0], L[1], L[2], R2, flag);
+}
 
 void launch_to_id_order(const DevView &v, cudaStream_t s, int r, int grid)
 {

@@ -166,25 +166,43 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
     }
 }
 
-// Warp per particle, FP64 exact arithmetic: E_i = sum over the 27-cell stencil
-// (j != i, r < rc, minimum image) in the canonical 32-way order; used for the
-// total energy (tot_ene, MCnptColloid.c:1598-1622) on any grid, including
-// boxes of fewer than 3 cells per axis.  With lam != 1 also the energy of the
-// configuration scaled by lam about the origin (NPT volume move), colloid at
-// the scaled box centre.  Outputs per particle slot: e0 (unscaled), e1 (scaled).
-__global__ void __launch_bounds__(128) k_energy_exact(DevView v, double *e0, double *e1, int *hard, int scaled)
+// Total energy (tot_ene, MCnptColloid.c:1598-1622) in FP64, warp per particle:
+// sum over unordered pairs (r < rc, minimum image) found in the 27-cell
+// stencil, plus the colloid term of every particle.  With lam != 1 also the
+// energy of the configuration scaled by lam about the origin (NPT volume
+// move), colloid at the scaled box centre.  Works on any grid, including boxes
+// of fewer than 3 cells per axis (the wrapped stencil is deduplicated).
+//
+// Each pair is evaluated once: slots are sorted by cell, so particle i takes
+// the rest of its own cell (slots > i) and the whole of every stencil cell
+// with a larger index; e0[i] (e1[i] scaled) holds those pair terms plus its
+// colloid term, and the slot sums add up to the total.  Only about one
+// candidate in eight is inside the cutoff, so pairs are not evaluated where
+// they are found: a distance pass over 32 candidates at a time appends the
+// in-cutoff (candidate, configuration) items to a per-warp queue, and every
+// 32 queued items are evaluated with all lanes busy.  The order of the FP64
+// additions is fixed by the data, so results repeat bit for bit.
+constexpr int EQ = 96; // queue entries per warp: < 32 pending + 64 from one chunk
+#ifndef LCMC_ENERGY_MIN_BLOCKS
+#define LCMC_ENERGY_MIN_BLOCKS 8
+#endif
+
+__global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(DevView v, double *e0, double *e1, int *hard, int scaled)
 {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int nw = blockDim.x >> 5;
-    __shared__ int s_cell[4][27];
-    __shared__ int s_base[4][28];
+    const unsigned lt = (1u << lane) - 1u;
+    __shared__ int s_start[4][28]; // flat index of the first candidate of each cell
+    __shared__ int s_base[4][28];  // particle slot minus flat index, per cell
+    __shared__ int s_qj[4][EQ];    // queued candidate slot, configuration in bit 31
     for (int i = blockIdx.x * nw + wib; i < v.ntot; i += gridDim.x * nw) {
         const int r = v.p2r[i];
         const Replica &p = v.rep[r];
         const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
         if (scaled && (p.ensemble != 2 || (p.da_on && !p.vol_stage1))) continue; // NVT, or screened out
-        const int cell = v.scid[i] - p.cell_off;
+        const int own = v.scid[i];
+        const int cell = own - p.cell_off;
         const int cx = cell % nc0, cy = (cell / nc0) % nc1, cz = cell / (nc0 * nc1);
         int c = -1;
         if (lane < 27) {
@@ -192,53 +210,98 @@ __global__ void __launch_bounds__(128) k_energy_exact(DevView v, double *e0, dou
             int x = (cx + dx + nc0) % nc0, y = (cy + dy + nc1) % nc1, z = (cz + dz + nc2) % nc2;
             c = p.cell_off + (z * nc1 + y) * nc0 + x;
         }
-        unsigned same = __match_any_sync(0xffffffffu, c);
-        bool keep = lane < 27 && (__ffs(same) - 1) == lane;
-        unsigned kb = __ballot_sync(0xffffffffu, keep);
-        int ncell = __popc(kb);
-        int slot = __popc(kb & ((1u << lane) - 1u));
-        if (keep) s_cell[wib][slot] = c;
-        __syncwarp();
-        int cnt_slot = 0;
-        if (lane < ncell) cnt_slot = v.cell_start[s_cell[wib][lane] + 1] - v.cell_start[s_cell[wib][lane]];
-        int inc = cnt_slot;
+        const unsigned same = __match_any_sync(0xffffffffu, c);
+        const bool keep = lane < 27 && (__ffs(same) - 1) == lane && c >= own;
+        const unsigned kb = __ballot_sync(0xffffffffu, keep);
+        const int ncell = __popc(kb);
+        const int slot = __popc(kb & lt);
+        int first = 0, cnt = 0;
+        if (keep) {
+            const int b = v.cell_start[c], e = v.cell_start[c + 1];
+            first = c == own ? i + 1 : b;
+            cnt = e - first;
+        }
+        int inc = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, inc, o);
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
             if (lane >= o) inc += y;
         }
-        if (lane < ncell) s_base[wib][lane] = inc - cnt_slot;
-        if (lane == 31) s_base[wib][ncell] = inc;
+        if (keep) {
+            s_start[wib][slot] = inc - cnt;
+            s_base[wib][slot] = first - (inc - cnt);
+        }
+        const int total = __shfl_sync(0xffffffffu, inc, 31);
+        if (lane == 0) s_start[wib][ncell] = total;
         __syncwarp();
 
         const double lam = scaled ? p.vol_lambda : 1.0;
         const double Ls[3] = {p.L[0] * lam, p.L[1] * lam, p.L[2] * lam};
-        double ri[3] = {v.px[i], v.py[i], v.pz[i]};
-        double ei[3] = {v.ox[i], v.oy[i], v.oz[i]};
-        double rs[3] = {ri[0] * lam, ri[1] * lam, ri[2] * lam};
+        const double ri[3] = {v.px[i], v.py[i], v.pz[i]};
+        const double ei[3] = {v.ox[i], v.oy[i], v.oz[i]};
+        const double rs[3] = {ri[0] * lam, ri[1] * lam, ri[2] * lam};
+        // the scaled distance is lam^2 r2 up to a few ulp: decide the scaled
+        // cutoff from it unless it lies within 1e-10 of rc^2
+        const double lam2 = lam * lam, rc2 = p.k.rc2, band = 1e-10 * rc2;
         double a0 = 0.0, a1 = 0.0;
-        for (int s = 0; s < ncell; s++) {
-            const int B = s_base[wib][s], n_s = s_base[wib][s + 1] - B;
-            const int g0 = v.cell_start[s_cell[wib][s]];
-            for (int q = B + ((lane - B) & 31); q < B + n_s; q += 32) {
-                const int j = g0 + (q - B);
-                if (j == i) continue;
-                double rj[3] = {v.px[j], v.py[j], v.pz[j]};
-                double ej[3] = {v.ox[j], v.oy[j], v.oz[j]};
+        int qn = 0;
+        int sc = 0; // this lane's current cell (its candidates only move forward)
+
+        for (int t0 = 0; t0 < total; t0 += 32) {
+            const int q = t0 + lane;
+            bool f0 = false, f1 = false;
+            int j = 0;
+            if (q < total) {
+                while (s_start[wib][sc + 1] <= q) sc++;
+                j = s_base[wib][sc] + q;
+                const double rj[3] = {v.px[j], v.py[j], v.pz[j]};
                 double d[3];
-                double r2 = dist_fold(ri[0], ri[1], ri[2], rj[0], rj[1], rj[2], p.L, d);
-                if (r2 < p.k.rc2) a0 += pair_exact(p.k, r2, d, ei, ej);
+                const double r2 = dist_fold(ri[0], ri[1], ri[2], rj[0], rj[1], rj[2], p.L, d);
+                f0 = r2 < rc2;
                 if (scaled) {
-                    double rjs[3] = {rj[0] * lam, rj[1] * lam, rj[2] * lam};
-                    r2 = dist_fold(rs[0], rs[1], rs[2], rjs[0], rjs[1], rjs[2], Ls, d);
-                    if (r2 < p.k.rc2) a1 += pair_exact(p.k, r2, d, ei, ej);
+                    const double r2s = lam2 * r2;
+                    if (fabs(r2s - rc2) > band) f1 = r2s < rc2;
+                    else f1 = dist_fold(rs[0], rs[1], rs[2], rj[0] * lam, rj[1] * lam, rj[2] * lam, Ls, d) < rc2;
                 }
+            }
+            const unsigned b0 = __ballot_sync(0xffffffffu, f0);
+            const unsigned b1 = __ballot_sync(0xffffffffu, f1);
+            if (f0) s_qj[wib][qn + __popc(b0 & lt)] = j;
+            if (f1) s_qj[wib][qn + __popc(b0) + __popc(b1 & lt)] = j | (int)0x80000000u;
+            qn += __popc(b0) + __popc(b1);
+            __syncwarp();
+            // evaluate full batches of 32 queued pairs
+            while (qn >= 32 || (qn > 0 && t0 + 32 >= total)) {
+                const int m = qn < 32 ? qn : 32;
+                if (lane < m) {
+                    const int e = s_qj[wib][lane];
+                    const int jj = e & 0x7fffffff;
+                    const double rj[3] = {v.px[jj], v.py[jj], v.pz[jj]};
+                    const double ej[3] = {v.ox[jj], v.oy[jj], v.oz[jj]};
+                    double d[3], r2;
+                    if (e < 0) {
+                        r2 = dist_fold(rs[0], rs[1], rs[2], rj[0] * lam, rj[1] * lam, rj[2] * lam, Ls, d);
+                        a1 += pair_exact(p.k, r2, d, ei, ej);
+                    } else {
+                        r2 = dist_fold(ri[0], ri[1], ri[2], rj[0], rj[1], rj[2], p.L, d);
+                        a0 += pair_exact(p.k, r2, d, ei, ej);
+                    }
+                }
+                // move entries [m, qn) to the front
+                int mv0 = 0, mv1 = 0;
+                if (m + lane < qn) mv0 = s_qj[wib][m + lane];
+                if (m + 32 + lane < qn) mv1 = s_qj[wib][m + 32 + lane];
+                __syncwarp();
+                if (m + lane < qn) s_qj[wib][lane] = mv0;
+                if (m + 32 + lane < qn) s_qj[wib][32 + lane] = mv1;
+                __syncwarp();
+                qn -= m;
             }
         }
         a0 = warp_sum_butterfly(a0);
         a1 = warp_sum_butterfly(a1);
         if (lane == 0) {
-            double u0 = 0.5 * a0, u1 = 0.5 * a1;
+            double u0 = a0, u1 = a1;
             if (p.k.coll_on) {
                 u0 += colloid_rod(p.k, ri, ei, p.L);
                 if (scaled) u1 += colloid_rod(p.k, rs, ei, Ls);
@@ -264,6 +327,16 @@ namespace lcmc {
 void launch_phase_exact(const DevView &v, cudaStream_t s, int ci, int grid)
 {
     k_phase_exact<<<grid, 128, 0, s>>>(v, ci);
+}
+
+int energy_exact_blocks_per_sm()
+{
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_energy_exact, 128, 0) != cudaSuccess || b < 1) {
+        cudaGetLastError();
+        b = 4;
+    }
+    return b;
 }
 
 void launch_energy_exact(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int scaled, int grid)

@@ -1,8 +1,8 @@
 """Learned volume-move screen and the P2 effective-sample-size measurement.
 
 * :class:`Surrogate` - the 4097 -> 128 -> 128 -> 1 MLP of liblcmc.so (BF16
-  tensor-core kernels), trained on (features, exact dU/N) samples that plain NPT
-  runs record;
+  tensor-core kernels), trained on (features, exact slope dU / (N delta))
+  samples that plain NPT runs record;
 * :func:`collect_samples` - run plain NPT replicas and record samples;
 * :func:`p2_series` / :func:`ess` - the per-sweep P2 series of a replica and its
   effective sample size (integrated autocorrelation time with Sokal's automatic
@@ -19,7 +19,8 @@ from ._lib import FP, N_FEATURES, check, lib
 
 
 class Surrogate:
-    """The surrogate network; predicts (dU / N) / scale from 4097 features."""
+    """The surrogate network; predicts the slope dU / (N delta) of a volume
+    move, divided by `scale`, from the 4097 features of an end point."""
 
     def __init__(self, max_batch=512, seed=1):
         h = C.c_void_p()
@@ -43,17 +44,18 @@ class Surrogate:
     def handle(self):
         return self._h
 
-    def fit(self, x, y_per_n, epochs=10, batch=256, lr=1e-3, seed=1, max_abs=50.0):
-        """Train on features x (n x 4097) and exact dU/N targets; targets are
-        divided by their standard deviation (kept as `scale`).  Samples with
-        |dU/N| > max_abs (moves into overlaps, which stage 2 rejects anyway)
-        are left out: their R^12 energies would swamp the squared loss."""
-        y = np.asarray(y_per_n, dtype=np.float64)
+    def fit(self, x, slope, epochs=10, batch=256, lr=1e-3, seed=1, max_abs=1000.0):
+        """Train on features x (n x 4097) and exact slopes dU / (N delta);
+        targets are divided by their standard deviation (kept as `scale`).
+        Samples with |slope| > max_abs (moves into overlaps, which stage 2
+        rejects anyway) are left out: their R^12 energies would swamp the
+        squared loss."""
+        y = np.asarray(slope, dtype=np.float64)
         keep = np.isfinite(y) & (np.abs(y) <= max_abs)
         x = np.ascontiguousarray(np.asarray(x)[keep], dtype=np.float32)
         y = y[keep]
         if len(y) == 0:
-            raise ValueError("no training sample with |dU/N| <= max_abs")
+            raise ValueError("no training sample with |slope| <= max_abs")
         self.scale = float(np.std(y)) or 1.0
         t = np.ascontiguousarray(y / self.scale, dtype=np.float32)
         loss = C.c_float()
@@ -63,7 +65,7 @@ class Surrogate:
         return loss.value
 
     def predict(self, x):
-        """dU / N predicted for each feature row."""
+        """Slope dU / (N delta) predicted for each feature row."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         out = np.zeros(len(x), dtype=np.float32)
         check(lib().lcmc_mlp_predict(self._h, x.ctypes.data_as(FP), len(x), out.ctypes.data_as(FP)))
@@ -72,7 +74,7 @@ class Surrogate:
 
 def collect_samples(system, n_sweeps, capacity=None):
     """Run `n_sweeps` sweeps of a GBSystem (NPT replicas, plain volume moves)
-    recording (features, exact dU/N) of every evaluated volume move."""
+    recording (features, exact dU / (N delta)) of every evaluated volume move."""
     system.record_volume_samples(capacity or n_sweeps * system.n_replicas)
     system.sweep(n_sweeps)
     x, y = system.get_volume_samples()

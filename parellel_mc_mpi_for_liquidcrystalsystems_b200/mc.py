@@ -93,15 +93,26 @@ class GBSystem:
         lattice uploaded to the device, FP64 total energy computed."""
         self._check(lib().lcmc_init_config(self._h, replica))
 
-    def upload(self, px, py, pz, ox, oy, oz, box, replica=0):
+    def upload(self, px, py, pz, ox, oy, oz, box, replica=0, energy=None):
+        """Copy a configuration to the device; the total energy is recomputed
+        in FP64, or taken from `energy` (the caller's running energy, as the
+        reference's attempt_monte_carlo_move carries it)."""
         arrs = [_dp(x) for x in (px, py, pz, ox, oy, oz)]
         b, bp = _dp(box)
         n = len(arrs[0][0])
-        self._check(lib().lcmc_upload(self._h, replica, *[p for _, p in arrs], n, bp))
+        if energy is None:
+            self._check(lib().lcmc_upload(self._h, replica, *[p for _, p in arrs], n, bp))
+        else:
+            self._check(lib().lcmc_upload_with_energy(self._h, replica, *[p for _, p in arrs], n, bp, float(energy)))
 
-    def download(self, replica=0):
+    def download(self, replica=0, out=None):
+        """(6 arrays in id order, box); `out` = 6 float64 arrays to fill (for
+        example pinned host buffers) instead of new ones."""
         n = self.params[replica].num_particles
-        out = [np.zeros(n) for _ in range(6)]
+        if out is None:
+            out = [np.empty(n) for _ in range(6)]
+        elif len(out) != 6 or any(a.dtype != np.float64 or a.shape != (n,) or not a.flags.c_contiguous for a in out):
+            raise ValueError("out must be 6 contiguous float64 arrays of num_particles")
         box = np.zeros(3)
         self._check(lib().lcmc_download(self._h, replica, *[x.ctypes.data_as(_lib.DP) for x in out], n,
                                         box.ctypes.data_as(_lib.DP)))
@@ -149,13 +160,13 @@ class GBSystem:
             self._surrogate = surrogate  # keep it alive while set
 
     def record_volume_samples(self, capacity):
-        """Record (features, exact dU / N) of the next `capacity` exactly
+        """Record (features, exact dU / (N delta)) of the next `capacity` exactly
         evaluated volume moves (0 stops and frees)."""
         self._check(lib().lcmc_record_volume_samples(self._h, capacity))
         self.samples_capacity = capacity
 
     def get_volume_samples(self):
-        """Recorded samples: features (n, 4097) float32 and dU / N (n,)."""
+        """Recorded samples: features (n, 4097) float32 and dU / (N delta) (n,)."""
         cap = getattr(self, "samples_capacity", 0)
         x = np.zeros((max(cap, 1), _lib.N_FEATURES), dtype=np.float32)
         y = np.zeros(max(cap, 1), dtype=np.float32)

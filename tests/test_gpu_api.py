@@ -1,0 +1,88 @@
+"""Host-boundary behaviour of the C ABI on the GPU.
+
+* a rejected upload (particle outside the box, inside the colloid, zero
+  orientation) returns its error and leaves the replica's state unchanged;
+* lcmc_upload_with_energy takes the caller's running energy in place of the
+  FP64 recompute and makes the same decisions as lcmc_upload;
+* download into caller-owned arrays.
+"""
+import numpy as np
+import pytest
+
+import parellel_mc_mpi_for_liquidcrystalsystems_b200 as lcmc
+from parellel_mc_mpi_for_liquidcrystalsystems_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+COMMON = dict(gb_kappa=3.0, gb_kappa_prime=5.0, gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
+              max_displacement=0.1, max_rotation=0.1)
+
+
+def bits(a):
+    return np.asarray(a, dtype=np.float64).view(np.uint64)
+
+
+def test_rejected_upload_keeps_the_state():
+    p = lcmc.default_params(num_particles=2000, system_density=0.30, rng_seed=3, colloid_wall_option=1,
+                            colloid_radius=3.0, **COMMON)
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(2)
+        (a, box) = s.download()
+        e = s.stats()["energy"]
+        cases = []
+        bad = [x.copy() for x in a]
+        bad[0][5] = -1.0
+        cases.append((bad, _lib.EINVAL))
+        bad = [x.copy() for x in a]
+        bad[0][7], bad[1][7], bad[2][7] = 0.5 * box[0], 0.5 * box[1], 0.5 * box[2] + 1.0
+        cases.append((bad, _lib.EOVERLAP))
+        bad = [x.copy() for x in a]
+        bad[3][9] = bad[4][9] = bad[5][9] = 0.0
+        cases.append((bad, _lib.EINVAL))
+        bad = [x.copy() for x in a]
+        bad[4][11] = np.nan
+        cases.append((bad, _lib.EINVAL))
+        for arrs, code in cases:
+            with pytest.raises(lcmc.LcmcError) as ei:
+                s.upload(*arrs, box)
+            assert ei.value.code == code
+            (b, box2) = s.download()
+            for u, v in zip(a, b):
+                assert np.array_equal(bits(u), bits(v))
+            assert np.array_equal(box, box2)
+            assert s.stats()["energy"] == e
+        s.sweep(1)  # the context still works
+
+
+def test_upload_with_energy_matches_upload():
+    p = lcmc.default_params(num_particles=4000, system_density=0.30, rng_seed=9, **COMMON)
+    a, box = lcmc.lattice(p)
+    with lcmc.GBSystem(p) as s1, lcmc.GBSystem(p) as s2:
+        s1.upload(*a, box)
+        e0 = s1.stats()["energy"]
+        s2.upload(*a, box, energy=e0 + 100.0)
+        assert s2.stats()["energy"] == e0 + 100.0
+        for _ in range(3):
+            s1.sweep(1)
+            s2.sweep(1)
+            assert np.array_equal(s1.outcomes(), s2.outcomes())
+        d1, d2 = s1.stats()["energy"], s2.stats()["energy"]
+        assert abs((d2 - d1) - 100.0) <= 1e-9 * max(1.0, abs(d1))
+        with pytest.raises(lcmc.LcmcError):
+            s2.upload(*a, box, energy=float("inf"))
+
+
+def test_download_into_caller_arrays():
+    p = lcmc.default_params(num_particles=1000, system_density=0.30, rng_seed=4, **COMMON)
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(1)
+        want, box = s.download()
+        out = [np.full(1000, -7.0) for _ in range(6)]
+        got, box2 = s.download(out=out)
+        assert all(g is o for g, o in zip(got, out))
+        for u, v in zip(want, out):
+            assert np.array_equal(bits(u), bits(v))
+        with pytest.raises(ValueError):
+            s.download(out=[np.zeros(999)] * 6)
