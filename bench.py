@@ -346,6 +346,34 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
         "seconds_total": time.perf_counter() - t_start}
 
 
+def npt_workload(lcmc, torch, n, steps, warmup):
+    """NPT sweeps of one system (colloid R = 8, T* = 0.85, P* = 2): a dilute
+    start compressed for 700 sweeps (dlnV_max 0.05), `warmup` sweeps at
+    dlnV_max = 0.01, then `steps` timed sweeps; device time per sweep by part."""
+    import numpy as np
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05)) as s:
+        st, box = dilute_start(n, 0.06, 8.0, 12)
+        s.upload(*st, box)
+        s.sweep(700)
+        st, box = s.download()
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01)) as s:
+        s.upload(*st, box)
+        s.sweep(max(3, warmup))
+        parts, total = [], 0.0
+        for _ in range(steps):
+            total += timed_sweeps(torch, s, 1)
+            parts.append(s.last_sweep_timing())
+        stt = s.stats()
+        parts = np.median(np.array(parts), axis=0)
+        return {"workload": f"NPT sweeps, N={n}, colloid R=8, T*=0.85, P*=2.0, dlnV_max=0.01, GB(3,5,2,1), FP32 "
+                            "sweep kernel, FP64 volume energies, compressed from a dilute lattice",
+                "steps": steps, "ms_per_sweep": 1e3 * total / steps,
+                "ms_parts_median": {"rebin": parts[0], "colour_phases": parts[1], "volume_move": parts[2],
+                                    "finalize": parts[3]},
+                "rho": n / float(np.prod(stt["box"])), "energy_per_particle": stt["energy"] / n,
+                "kernels_per_sweep": s.kernels_per_sweep()}
+
+
 # ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -358,6 +386,9 @@ def main():
     ap.add_argument("--da-sweeps", type=int, default=4000,
                     help="sweeps per arm of the NPT delayed-acceptance measurement (0 skips it)")
     ap.add_argument("--da-train-sweeps", type=int, default=400)
+    ap.add_argument("--workload", default="moves", choices=["moves", "npt"],
+                    help="npt: time NPT sweeps of one compressed system (per-part device times) instead")
+    ap.add_argument("--npt-n", type=int, default=262144)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -387,6 +418,10 @@ def main():
     import parellel_mc_mpi_for_liquidcrystalsystems_b200 as lcmc
 
     torch.cuda.set_device(local)
+    if args.workload == "npt":
+        if rank == 0:
+            print(json.dumps(npt_workload(lcmc, torch, args.npt_n, args.steps, args.warmup)))
+        return 0
     dist = None
     if world > 1:
         import datetime

@@ -204,3 +204,34 @@ double refdrv_run_attempts(long n_attempts, int rebuild, double *px, double *py,
     *rebuilds = nreb;
     return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
 }
+
+/*
+ * As refdrv_run_attempts, for ensemble averages: the Verlet list (cell-built,
+ * same content as build_neighbor_lists) is rebuilt every `period` attempts
+ * instead of by the reference's tracker (which sums the rotation-table
+ * magnitude, not the real displacement, MCnptColloid.c:2584-2595), so the
+ * old energies of GBij_lstnb stay exact when period * max_displacement is
+ * small against the skin verlet_radius - cutoff_radius.  The energy is
+ * recomputed (tot_ene_lstnb) after every rebuild.
+ */
+double refdrv_run_attempts_periodic(long n_attempts, long period, double *px, double *py, double *pz, double *ox,
+                                    double *oy, double *oz, int *count, int *list, long list_cap, double *energy,
+                                    long *accepted)
+{
+    size_t *hist = calloc((size_t)num_particles, sizeof(size_t));
+    double tracker = 0.0;
+    long acc = 0;
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    for (long c = 0; c < n_attempts; c++) {
+        if (c % period == 0) {
+            if (refdrv_build_verlet_cells(px, py, pz, count, list, list_cap) < 0) break;
+            *energy = tot_ene_lstnb(px, py, pz, ox, oy, oz, count, list);
+        }
+        attempt_monte_carlo_move(px, py, pz, ox, oy, oz, max_displacement, energy, count, list, &acc, &tracker, hist);
+    }
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    free(hist);
+    *accepted += acc;
+    return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+}

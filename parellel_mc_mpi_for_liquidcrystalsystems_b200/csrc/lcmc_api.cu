@@ -632,8 +632,9 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     ALLOC(c->d_phard, c->ntot);
     ALLOC(c->d_red, 16 * n + 16);
     {
-        int nmax = 1;
-        for (int r = 0; r < n; r++) nmax = std::max(nmax, params[r].num_particles);
+        int nmax = 1; // largest count a chunked sum covers: particles or cells of a replica
+        for (int r = 0; r < n; r++)
+            nmax = std::max(nmax, std::max(params[r].num_particles, c->rep[r].nc_max * c->rep[r].nc_max * c->rep[r].nc_max));
         c->red_nchunk = (nmax + LCMC_RED_CHUNK - 1) / LCMC_RED_CHUNK;
     }
     ALLOC(c->d_red_part, (size_t)n * c->red_nchunk * 6);
@@ -845,8 +846,8 @@ extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
     if (!ctx) return LCMC_EINVAL;
     // rebin: setup, bin, 3 scan, scatter, sort, gather; phases; volume: propose, energy, chunk sums, accept,
     // scale; surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1; recording; history: chunk sums,
-    // rows; finalize
-    int n = 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 1;
+    // rows; finalize: chunk sums, statistics
+    int n = 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 2;
     if (ctx->any_npt && (ctx->any_da || ctx->rec_cap > 0)) n += 2;
     if (ctx->any_npt && ctx->any_da) n += 6;
     if (ctx->any_npt && ctx->rec_cap > 0) n += 1;

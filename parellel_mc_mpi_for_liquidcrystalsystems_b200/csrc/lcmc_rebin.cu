@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "lcmc_internal.h"
+#include "lcmc_reduce.cuh"
 #include "lcmc_rng.cuh"
 #include "lcmc_trial.cuh"
 
@@ -259,49 +260,48 @@ __global__ void k_gather(DevView v)
 
 // Block per replica: deterministic sums of the per-cell sweep results
 // (accepted dE, accepted count, hard-core rejects, pair/candidate counters).
-__global__ void k_sweep_finalize(DevView v)
+// Per-cell results of a sweep in chunks of LCMC_RED_CHUNK cells (blocks:
+// chunk, replica): dE, accepted, hard-core rejections, in-cutoff pairs and
+// stencil candidates (counts are exact in FP64).
+__global__ void __launch_bounds__(256) k_cell_chunk_sums(DevView v)
 {
-    int r = blockIdx.x;
+    const int c = blockIdx.x, r = blockIdx.y;
+    const Replica &p = v.rep[r];
+    const int ncell = p.nc[0] * p.nc[1] * p.nc[2];
+    const int i0 = c * LCMC_RED_CHUNK;
+    if (i0 >= ncell) return;
+    const int i1 = min(ncell, i0 + LCMC_RED_CHUNK);
+    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = i0 + (int)threadIdx.x; i < i1; i += blockDim.x) {
+        const int g = p.cell_off + i;
+        s[0] += v.cell_e0[g];
+        s[1] += (double)v.cell_n0[g];
+        s[2] += (double)v.cell_n1[g];
+        s[3] += (double)v.cell_pairs[g];
+        s[4] += (double)v.cell_cands[g];
+    }
+    __shared__ double sh[5][8];
+    block_sums<5>(s, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; k++) v.red_part[((size_t)r * v.red_nchunk + c) * 6 + k] = s[k];
+}
+
+// Block per replica: add the chunk sums into the statistics, count the sweep.
+__global__ void __launch_bounds__(256) k_sweep_finalize(DevView v)
+{
+    const int r = blockIdx.x;
     Replica &p = v.rep[r];
-    int c0 = p.cell_off, nc = p.nc[0] * p.nc[1] * p.nc[2];
-    double e = 0.0;
-    long long na = 0, nh = 0;
-    unsigned long long np = 0, ncand = 0;
-    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
-        e += v.cell_e0[c0 + c];
-        na += v.cell_n0[c0 + c];
-        nh += v.cell_n1[c0 + c];
-        np += v.cell_pairs[c0 + c];
-        ncand += v.cell_cands[c0 + c];
-    }
-    __shared__ double se[256];
-    __shared__ long long sa[256], sh_[256];
-    __shared__ unsigned long long sp[256], sc[256];
-    se[threadIdx.x] = e;
-    sa[threadIdx.x] = na;
-    sh_[threadIdx.x] = nh;
-    sp[threadIdx.x] = np;
-    sc[threadIdx.x] = ncand;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) {
-            se[threadIdx.x] += se[threadIdx.x + o];
-            sa[threadIdx.x] += sa[threadIdx.x + o];
-            sh_[threadIdx.x] += sh_[threadIdx.x + o];
-            sp[threadIdx.x] += sp[threadIdx.x + o];
-            sc[threadIdx.x] += sc[threadIdx.x + o];
-        }
-        __syncthreads();
-    }
+    double s[5];
+    finish_sums<5>(v, r, p.nc[0] * p.nc[1] * p.nc[2], s);
     if (threadIdx.x == 0) {
-        DevStats &s = v.stats[r];
-        s.attempted += (unsigned long long)p.n;
-        s.accepted += (unsigned long long)sa[0];
-        s.hard += (unsigned long long)sh_[0];
-        s.pairs += sp[0];
-        s.cands += sc[0];
-        s.energy += se[0];
-        if (!(se[0] == se[0]) || se[0] - se[0] != 0.0) s.flags |= F_NONFINITE;
+        DevStats &st = v.stats[r];
+        st.attempted += (unsigned long long)p.n;
+        st.accepted += (unsigned long long)s[1];
+        st.hard += (unsigned long long)s[2];
+        st.pairs += (unsigned long long)s[3];
+        st.cands += (unsigned long long)s[4];
+        st.energy += s[0];
+        if (!(s[0] == s[0]) || s[0] - s[0] != 0.0) st.flags |= F_NONFINITE;
         p.sweep += 1ull;
     }
 }
@@ -326,6 +326,10 @@ void launch_rebin(const DevView &v, cudaStream_t s, int grid)
     k_gather<<<grid, 256, 0, s>>>(v);
 }
 
-void launch_finalize(const DevView &v, cudaStream_t s) { k_sweep_finalize<<<v.R, 256, 0, s>>>(v); }
+void launch_finalize(const DevView &v, cudaStream_t s)
+{
+    k_cell_chunk_sums<<<dim3(v.red_nchunk, v.R), 256, 0, s>>>(v);
+    k_sweep_finalize<<<v.R, 256, 0, s>>>(v);
+}
 
 } // namespace lcmc

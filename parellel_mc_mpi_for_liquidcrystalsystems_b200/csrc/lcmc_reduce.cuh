@@ -29,18 +29,24 @@ __device__ __forceinline__ void block_sums(double (&s)[K], double (*sh)[8])
     __syncthreads();
 }
 
-// Sum of replica r's chunk partials (call from every thread of one block;
-// thread 0 holds the result).
+// Sum of replica r's chunk partials over `count` items (particles by
+// default; call from every thread of one block; thread 0 holds the result).
 template <int K>
-__device__ __forceinline__ void finish_sums(const DevView &v, int r, double (&s)[K])
+__device__ __forceinline__ void finish_sums(const DevView &v, int r, int count, double (&s)[K])
 {
-    const int nc = (v.rep[r].n + LCMC_RED_CHUNK - 1) / LCMC_RED_CHUNK;
+    const int nc = (count + LCMC_RED_CHUNK - 1) / LCMC_RED_CHUNK;
 #pragma unroll
     for (int k = 0; k < K; k++) s[k] = 0.0;
     for (int c = threadIdx.x; c < nc; c += blockDim.x)
         for (int k = 0; k < K; k++) s[k] += v.red_part[((size_t)r * v.red_nchunk + c) * 6 + k];
     __shared__ double sh[K][8];
     block_sums<K>(s, sh);
+}
+
+template <int K>
+__device__ __forceinline__ void finish_sums(const DevView &v, int r, double (&s)[K])
+{
+    finish_sums<K>(v, r, v.rep[r].n, s);
 }
 
 } // namespace lcmc

@@ -168,10 +168,12 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
 
 // Total energy (tot_ene, MCnptColloid.c:1598-1622) in FP64, warp per particle:
 // sum over unordered pairs (r < rc, minimum image) found in the 27-cell
-// stencil, plus the colloid term of every particle.  With lam != 1 also the
-// energy of the configuration scaled by lam about the origin (NPT volume
-// move), colloid at the scaled box centre.  Works on any grid, including boxes
-// of fewer than 3 cells per axis (the wrapped stencil is deduplicated).
+// stencil, plus the colloid term of every particle, with pair_exact (the
+// reference-order term).  SCALED: the NPT volume move's energies of the
+// current configuration and of the one scaled by lam about the origin
+// (colloid at the scaled box centre), with pair_energy64.  Works on any grid,
+// including boxes of fewer than 3 cells per axis (the wrapped stencil is
+// deduplicated).
 //
 // Each pair is evaluated once: slots are sorted by cell, so particle i takes
 // the rest of its own cell (slots > i) and the whole of every stencil cell
@@ -187,7 +189,8 @@ constexpr int EQ = 96; // queue entries per warp: < 32 pending + 64 from one chu
 #define LCMC_ENERGY_MIN_BLOCKS 8
 #endif
 
-__global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(DevView v, double *e0, double *e1, int *hard, int scaled)
+template <bool SCALED>
+__global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(DevView v, double *e0, double *e1, int *hard)
 {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(De
         const int r = v.p2r[i];
         const Replica &p = v.rep[r];
         const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
-        if (scaled && (p.ensemble != 2 || (p.da_on && !p.vol_stage1))) continue; // NVT, or screened out
+        if (SCALED && (p.ensemble != 2 || (p.da_on && !p.vol_stage1))) continue; // NVT, or screened out
         const int own = v.scid[i];
         const int cell = own - p.cell_off;
         const int cx = cell % nc0, cy = (cell / nc0) % nc1, cz = cell / (nc0 * nc1);
@@ -235,7 +238,7 @@ __global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(De
         if (lane == 0) s_start[wib][ncell] = total;
         __syncwarp();
 
-        const double lam = scaled ? p.vol_lambda : 1.0;
+        const double lam = SCALED ? p.vol_lambda : 1.0;
         const double Ls[3] = {p.L[0] * lam, p.L[1] * lam, p.L[2] * lam};
         const double ri[3] = {v.px[i], v.py[i], v.pz[i]};
         const double ei[3] = {v.ox[i], v.oy[i], v.oz[i]};
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(De
                 double d[3];
                 const double r2 = dist_fold(ri[0], ri[1], ri[2], rj[0], rj[1], rj[2], p.L, d);
                 f0 = r2 < rc2;
-                if (scaled) {
+                if (SCALED) {
                     const double r2s = lam2 * r2;
                     if (fabs(r2s - rc2) > band) f1 = r2s < rc2;
                     else f1 = dist_fold(rs[0], rs[1], rs[2], rj[0] * lam, rj[1] * lam, rj[2] * lam, Ls, d) < rc2;
@@ -281,10 +284,10 @@ __global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(De
                     double d[3], r2;
                     if (e < 0) {
                         r2 = dist_fold(rs[0], rs[1], rs[2], rj[0] * lam, rj[1] * lam, rj[2] * lam, Ls, d);
-                        a1 += pair_exact(p.k, r2, d, ei, ej);
+                        a1 += pair_energy64(p.k, r2, d, ei, ej);
                     } else {
                         r2 = dist_fold(ri[0], ri[1], ri[2], rj[0], rj[1], rj[2], p.L, d);
-                        a0 += pair_exact(p.k, r2, d, ei, ej);
+                        a0 += SCALED ? pair_energy64(p.k, r2, d, ei, ej) : pair_exact(p.k, r2, d, ei, ej);
                     }
                 }
                 // move entries [m, qn) to the front
@@ -304,10 +307,10 @@ __global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(De
             double u0 = a0, u1 = a1;
             if (p.k.coll_on) {
                 u0 += colloid_rod(p.k, ri, ei, p.L);
-                if (scaled) u1 += colloid_rod(p.k, rs, ei, Ls);
+                if (SCALED) u1 += colloid_rod(p.k, rs, ei, Ls);
             }
             e0[i] = u0;
-            if (scaled) {
+            if (SCALED) {
                 e1[i] = u1;
                 double d[3];
                 double r2 = dist_fold(rs[0], rs[1], rs[2], 0.5 * Ls[0], 0.5 * Ls[1], 0.5 * Ls[2], Ls, d);
@@ -332,7 +335,7 @@ void launch_phase_exact(const DevView &v, cudaStream_t s, int ci, int grid)
 int energy_exact_blocks_per_sm()
 {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_energy_exact, 128, 0) != cudaSuccess || b < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_energy_exact<true>, 128, 0) != cudaSuccess || b < 1) {
         cudaGetLastError();
         b = 4;
     }
@@ -341,7 +344,8 @@ int energy_exact_blocks_per_sm()
 
 void launch_energy_exact(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int scaled, int grid)
 {
-    k_energy_exact<<<grid, 128, 0, s>>>(v, e0, e1, hard, scaled);
+    if (scaled) k_energy_exact<true><<<grid, 128, 0, s>>>(v, e0, e1, hard);
+    else k_energy_exact<false><<<grid, 128, 0, s>>>(v, e0, e1, hard);
 }
 
 } // namespace lcmc

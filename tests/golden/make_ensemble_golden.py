@@ -1,0 +1,121 @@
+#!/usr/bin/env python3
+"""Ensemble averages from the reference's OWN Monte Carlo chain.
+
+Runs in a container where the reference source is available: loads
+oracle/_ref/libmcref_serial.so (MCnptColloid.c built by oracle/build_ref.sh)
+and runs attempt_monte_carlo_move (MCnptColloid.c:2445-2604, random particle
+per attempt, libc rand()) from the seeded lattice of the oracle, with the
+Verlet list rebuilt every N attempts (refdrv_run_attempts_periodic).  After a
+burn-in it records U/N (the reference's running energy) and P2 (largest
+eigenvalue of the Q tensor, in numpy) after every N attempts, and stores the
+means with block-averaged standard errors in ensemble_golden.npz.
+
+System: N = 1728 Gay-Berne rods GB(3, 5, 2, 1), rho* = 0.10, T* = 1.0,
+r_c = 4.0, r_v = 5.0, d = 0.1, rotation 0.1, NVT, colloid of radius 2 at the
+box centre (colloid_wall_option 1, so the reference's ungated colloid term in
+moves and ours agree).  An isotropic fluid that relaxes from the lattice.
+"""
+import ctypes as C
+import os
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(HERE))
+REF_SO = os.path.join(REPO, "oracle", "_ref", "libmcref_serial.so")
+
+N, RHO, T, R_COLL, SEED = 1728, 0.10, 1.0, 2.0, 4242
+BURN, SWEEPS, BLOCKS = 1000, 10000, 20
+
+PARAM_TEXT = f"""# written by tests/golden/make_ensemble_golden.py
+mc_ensemble_type 1
+num_particles {N}
+system_density {RHO}
+system_temperature {T}
+system_pressure 1.0
+gb_sigma_sidetoside 1.0
+gb_epsilon0 1.0
+gb_kappa 3.0
+gb_kappa_prime 5.0
+gb_mu_exponent 2.0
+gb_nu_exponent 1.0
+max_displacement 0.1
+max_rotation 0.1
+initial_configuration_type 2
+cutoff_radius 4.0
+verlet_radius 5.0
+total_mc_cycles 1000
+configuration_save_interval 100
+statistics_print_interval 100
+colloid_wall_option 1
+colloid_interaction_epsilon 15
+colloid_interaction_amplitude 1.5
+colloid_radius {R_COLL}
+"""
+
+D, DP, IP = C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_int)
+
+
+def p2_of(ox, oy, oz):
+    u = np.stack([ox, oy, oz], 1)
+    u = u / np.linalg.norm(u, axis=1)[:, None]
+    Q = 1.5 * (u.T @ u) / len(u) - 0.5 * np.eye(3)
+    return float(np.linalg.eigvalsh(Q)[-1])
+
+
+def block_mean_se(x, blocks):
+    b = np.array_split(np.asarray(x), blocks)
+    m = np.array([v.mean() for v in b])
+    return float(m.mean()), float(m.std(ddof=1) / np.sqrt(blocks))
+
+
+def main():
+    import oracle_ctypes as oc
+    ref = C.CDLL(REF_SO)
+    ref.load_initial_conditions.argtypes = [C.c_char_p]
+    ref.refdrv_set_box.argtypes = [C.c_int, DP]
+    ref.refdrv_run_attempts_periodic.argtypes = [C.c_long, C.c_long, DP, DP, DP, DP, DP, DP, IP, IP, C.c_long, DP,
+                                                 C.POINTER(C.c_long)]
+    ref.refdrv_run_attempts_periodic.restype = D
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(PARAM_TEXT)
+        path = f.name
+    ref.load_initial_conditions(path.encode())
+    os.unlink(path)
+    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=N, rho=RHO, R=R_COLL, seed=SEED)
+    state = [np.ascontiguousarray(a, dtype=np.float64) for a in (px, py, pz, ox, oy, oz)]
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    ref.refdrv_set_box(N, box.ctypes.data_as(DP))
+    C.CDLL("libc.so.6").srand(SEED)
+    ref.refdrv_fill_rotation_table()
+    ptrs = [a.ctypes.data_as(DP) for a in state]
+    cap = 400 * N
+    cnt = np.zeros(N, dtype=np.int32)
+    lst = np.zeros(cap, dtype=np.int32)
+    E = D(0.0)
+    acc = C.c_long(0)
+    t0 = time.time()
+    args = (*ptrs, cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap, C.byref(E), C.byref(acc))
+    ref.refdrv_run_attempts_periodic(BURN * N, N, *args)
+    acc.value = 0
+    u, p2 = np.empty(SWEEPS), np.empty(SWEEPS)
+    for s in range(SWEEPS):
+        ref.refdrv_run_attempts_periodic(N, N, *args)
+        u[s] = E.value / N
+        p2[s] = p2_of(state[3], state[4], state[5])
+    mu, su = block_mean_se(u, BLOCKS)
+    mp, sp = block_mean_se(p2, BLOCKS)
+    out = os.path.join(HERE, "ensemble_golden.npz")
+    np.savez(out, n=N, rho=RHO, T=T, colloid_R=R_COLL, seed=SEED, burn=BURN, sweeps=SWEEPS, blocks=BLOCKS,
+             u_mean=mu, u_se=su, p2_mean=mp, p2_se=sp, acceptance=acc.value / (SWEEPS * N),
+             u_series=u[::10], p2_series=p2[::10])
+    print(f"U/N = {mu:.6f} +- {su:.6f}  P2 = {mp:.6f} +- {sp:.6f}  acceptance {acc.value / (SWEEPS * N):.3f}  "
+          f"in {time.time() - t0:.0f} s -> {out}")
+
+
+if __name__ == "__main__":
+    main()
