@@ -27,14 +27,16 @@
 //              grown by rc + max_displacement/2; warp w compacts its quarter of
 //              the candidates into its own segment (no block barrier per round)
 //   4 tasks    warps take tasks from a shared queue:
-//              particle task k: cutoff test of all staged candidates against
-//                k's old position with radius rc + |displacement| (covers old
-//                and new state), ballot compaction into the warp's list, then
-//                FP32 Gay-Berne for old and new state over the list, lane sums
-//                in FP64
+//              particle task (two particles k, k + 1): cutoff test of every
+//                staged candidate, loaded once, against both old positions
+//                with radius rc + |displacement| (covers old and new state),
+//                ballot compaction into two lists, then FP32 Gay-Berne for old
+//                and new state over both lists together, lane sums in FP64
 //              pair task: 32 unordered in-cell pairs, 4 terms each
 //              (old/new x old/new), differences formed in FP64
-//   5 sums     warp per particle: in-cell row sums -> dE before corrections
+//   5 sums     warp 0, thread per particle: in-cell row sums -> dE before the
+//              corrections (per-particle trial data was prefetched into
+//              shared memory in step 2)
 //   6 scan     warp 0: Metropolis decisions in id order with the corrections
 //   7 write    accepted trial states to the FP64 master arrays
 #include <cuda_runtime.h>
@@ -77,12 +79,17 @@ struct FastSmem {
     float4 cpos[NW * SEG];     // x, y, z, ux of the static candidates (segment per warp)
     float2 cori[NW * SEG];     // uy, uz
     float pCA[NPAIR], pBA[NPAIR], pcm[NPAIR]; // in-cell: C-A, B-A, (D-C)-(B-A)
-    float ax[AMAX], ay[AMAX], az[AMAX], aux[AMAX], auy[AMAX], auz[AMAX]; // old, relative
-    float bx[AMAX], by[AMAX], bz[AMAX], bux[AMAX], buy[AMAX], buz[AMAX]; // new, relative
+    // old (a) and trial (b) state of each active particle, relative to the cell
+    // origin: [0] = (ax, ay, az, aux), [1] = (auy, auz, bx, by), [2] = (bz, bux, buy, buz)
+    float4 pst[AMAX][3];
     float rad2[AMAX];
-    double Sold[AMAX], Snew[AMAX], dEk[AMAX];
+    double Sold[AMAX], Snew[AMAX];
+    double tn[6][AMAX];   // trial state (FP64 master values written on acceptance)
+    double tdU[AMAX], tlu[AMAX]; // colloid dU of the trial, log of the Metropolis draw
+    int pid[AMAX];        // particle id (outcome slot)
+    unsigned char hard[AMAX];
     int acc[AMAX];
-    unsigned short wlist[NW][LW];
+    unsigned short wlist[NW][2][LW]; // per warp: candidate lists of the task's two particles
     int st_start[27], st_cnt[27], st_pre[28];
     int segcnt[NW];
     int task;
@@ -124,6 +131,7 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
 {
     using SM = FastSmem<NT, AMAX, SEG, LW>;
     constexpr int NW = SM::NW;
+    static_assert(AMAX <= 64, "the scan warp holds two particles per lane");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SM &sm = *reinterpret_cast<SM *>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -201,20 +209,23 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             const double ex = v.ox[g], ey = v.oy[g], ez = v.oz[g];
             const float en = rsqrtf((float)(ex * ex + ey * ey + ez * ez));
             const float dx = v.tdx[g], dy = v.tdy[g], dz = v.tdz[g];
-            sm.ax[k] = (float)qx;
-            sm.ay[k] = (float)qy;
-            sm.az[k] = (float)qz;
-            sm.aux[k] = (float)ex * en;
-            sm.auy[k] = (float)ey * en;
-            sm.auz[k] = (float)ez * en;
-            sm.bx[k] = (float)qx + dx;
-            sm.by[k] = (float)qy + dy;
-            sm.bz[k] = (float)qz + dz;
-            sm.bux[k] = (float)v.tux[g];
-            sm.buy[k] = (float)v.tuy[g];
-            sm.buz[k] = (float)v.tuz[g];
+            const float ax = (float)qx, ay = (float)qy, az = (float)qz;
+            sm.pst[k][0] = make_float4(ax, ay, az, (float)ex * en);
+            sm.pst[k][1] = make_float4((float)ey * en, (float)ez * en, ax + dx, ay + dy);
+            sm.pst[k][2] = make_float4(az + dz, (float)v.tux[g], (float)v.tuy[g], (float)v.tuz[g]);
             const float rr = rcf + sqrtf(dx * dx + dy * dy + dz * dz) + 1e-3f;
-            sm.rad2[k] = v.thard[g] ? -1.0f : rr * rr;
+            const unsigned char hd = v.thard[g];
+            sm.rad2[k] = hd ? -1.0f : rr * rr;
+            sm.hard[k] = hd;
+            sm.tn[0][k] = v.tnx[g];
+            sm.tn[1][k] = v.tny[g];
+            sm.tn[2][k] = v.tnz[g];
+            sm.tn[3][k] = v.tux[g];
+            sm.tn[4][k] = v.tuy[g];
+            sm.tn[5][k] = v.tuz[g];
+            sm.tdU[k] = v.tdU[g];
+            sm.tlu[k] = v.tlu[g];
+            sm.pid[k] = v.id[g];
         }
 
         // ---- 3 staging: warp w takes a contiguous quarter of the 26 static cells'
@@ -225,43 +236,52 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             const float prune2 = K.rc2 * 1.0002f + 1e-3f;
             const int fb = (int)(((long long)S26 * w) / NW), fe = (int)(((long long)S26 * (w + 1)) / NW);
             int cnt = 0;
-            for (int base = fb; base < fe; base += 32) {
-                const int f = base + lane;
-                bool keep = false;
-                float x = 0, y = 0, z = 0, ux = 0, uy = 0, uz = 0;
-                if (f < fe) {
-                    // largest stencil slot whose prefix is <= f (slot 13 has an empty range;
-                    // an empty slot's prefix is the end of the previous range, so it is never picked)
-                    int s = 0, hi = 27;
-                    while (hi - s > 1) {
-                        const int mid = (s + hi) >> 1;
-                        if (sm.st_pre[mid] <= f) s = mid;
-                        else hi = mid;
-                    }
-                    const int g = sm.st_start[s] + (f - sm.st_pre[s]);
-                    // stencil offset of slot s is (s % 3, s / 3 % 3, s / 9) - 1
-                    x = (float)fold_rel(v.px[g], o0, ((double)(s % 3) - 0.5) * w0, L0, iL0);
-                    y = (float)fold_rel(v.py[g], o1, ((double)((s / 3) % 3) - 0.5) * w1, L1, iL1);
-                    z = (float)fold_rel(v.pz[g], o2, ((double)(s / 9) - 0.5) * w2, L2, iL2);
-                    const float qx = fmaxf(fmaxf(-hb - x, x - (wx + hb)), 0.0f);
-                    const float qy = fmaxf(fmaxf(-hb - y, y - (wy + hb)), 0.0f);
-                    const float qz = fmaxf(fmaxf(-hb - z, z - (wz + hb)), 0.0f);
-                    keep = qx * qx + qy * qy + qz * qz < prune2;
-                    if (keep) {
+            // two candidates per lane per round, all six coordinates loaded at
+            // once: the global loads of a round are independent of each other
+            for (int base = fb; base < fe; base += 64) {
+                float x[2], y[2], z[2], ux[2], uy[2], uz[2];
+                bool keep[2];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int f = base + 32 * h + lane;
+                    keep[h] = false;
+                    x[h] = y[h] = z[h] = ux[h] = uy[h] = uz[h] = 0.0f;
+                    if (f < fe) {
+                        // largest stencil slot whose prefix is <= f (slot 13 has an empty range;
+                        // an empty slot's prefix is the end of the previous range, so it is never picked)
+                        int sl = 0, hi = 27;
+                        while (hi - sl > 1) {
+                            const int mid = (sl + hi) >> 1;
+                            if (sm.st_pre[mid] <= f) sl = mid;
+                            else hi = mid;
+                        }
+                        const int g = sm.st_start[sl] + (f - sm.st_pre[sl]);
+                        const double gx = v.px[g], gy = v.py[g], gz = v.pz[g];
                         const double ex = v.ox[g], ey = v.oy[g], ez = v.oz[g];
+                        // stencil offset of slot sl is (sl % 3, sl / 3 % 3, sl / 9) - 1
+                        x[h] = (float)fold_rel(gx, o0, ((double)(sl % 3) - 0.5) * w0, L0, iL0);
+                        y[h] = (float)fold_rel(gy, o1, ((double)((sl / 3) % 3) - 0.5) * w1, L1, iL1);
+                        z[h] = (float)fold_rel(gz, o2, ((double)(sl / 9) - 0.5) * w2, L2, iL2);
+                        const float qx = fmaxf(fmaxf(-hb - x[h], x[h] - (wx + hb)), 0.0f);
+                        const float qy = fmaxf(fmaxf(-hb - y[h], y[h] - (wy + hb)), 0.0f);
+                        const float qz = fmaxf(fmaxf(-hb - z[h], z[h] - (wz + hb)), 0.0f);
+                        keep[h] = qx * qx + qy * qy + qz * qz < prune2;
                         const float in = rsqrtf((float)(ex * ex + ey * ey + ez * ez));
-                        ux = (float)ex * in;
-                        uy = (float)ey * in;
-                        uz = (float)ez * in;
+                        ux[h] = (float)ex * in;
+                        uy[h] = (float)ey * in;
+                        uz[h] = (float)ez * in;
                     }
                 }
-                const unsigned bal = __ballot_sync(0xffffffffu, keep);
-                const int pos = cnt + __popc(bal & lt);
-                if (keep && pos < SEG) {
-                    sm.cpos[w * SEG + pos] = make_float4(x, y, z, ux);
-                    sm.cori[w * SEG + pos] = make_float2(uy, uz);
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const unsigned bal = __ballot_sync(0xffffffffu, keep[h]);
+                    const int pos = cnt + __popc(bal & lt);
+                    if (keep[h] && pos < SEG) {
+                        sm.cpos[w * SEG + pos] = make_float4(x[h], y[h], z[h], ux[h]);
+                        sm.cori[w * SEG + pos] = make_float2(uy[h], uz[h]);
+                    }
+                    cnt += __popc(bal);
                 }
-                cnt += __popc(bal);
             }
             if (lane == 0) {
                 sm.segcnt[w] = cnt < SEG ? cnt : SEG;
@@ -279,83 +299,132 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
 #pragma unroll
         for (int i = 0; i < NW; i++) segc[i] = sm.segcnt[i];
 
-        // ---- 4 task queue: particle tasks (test + pair sums) and in-cell pair tasks ----
+        // ---- 4 task queue: particle tasks (two particles each: cutoff test +
+        //      pair sums) and in-cell pair tasks ----
+        // staged candidates as one flat index f over the warp segments:
+        // slot = f - segoff[i] for the segment i holding f
+        int segp[NW], segoff[NW];
+        {
+            int acc_ = 0;
+#pragma unroll
+            for (int i = 0; i < NW; i++) {
+                segp[i] = acc_;
+                segoff[i] = acc_ - i * SEG;
+                acc_ += segc[i];
+            }
+        }
+        const int stot = segp[NW - 1] + segc[NW - 1];
+        const int nptask = (na + 1) >> 1;
         const int npair = na * (na - 1) / 2;
-        const int ntask = na + (npair + 31) / 32;
+        const int ntask = nptask + (npair + 31) / 32;
         unsigned long long npairs = 0ull;
         for (;;) {
             int task = 0;
             if (lane == 0) task = atomicAdd(&sm.task, 1);
             task = __shfl_sync(0xffffffffu, task, 0);
             if (task >= ntask) break;
-            if (task < na) {
-                const int k = task;
-                const float R2 = sm.rad2[k];
-                double so = 0.0, sn = 0.0;
+            if (task < nptask) {
+                const int ka = 2 * task, kb = 2 * task + 1;
+                const bool has_b = kb < na;
+                const float R2a = sm.rad2[ka];
+                const float R2b = has_b ? sm.rad2[kb] : -1.0f;
+                const float4 qa = sm.pst[ka][0];
+                const float4 qb = has_b ? sm.pst[kb][0] : qa;
+                double soa = 0.0, sna = 0.0, sob = 0.0, snb = 0.0;
                 int np = 0;
-                if (R2 > 0.0f) {
-                    const float xo = sm.ax[k], yo = sm.ay[k], zo = sm.az[k];
-                    int cnt = 0;
+                if (R2a > 0.0f || R2b > 0.0f) {
+                    int ca = 0, cb = 0;
+                    for (int base = 0; base < stot; base += 64) {
+                        bool pa[2], pb[2];
+                        int sl[2];
 #pragma unroll
-                    for (int sg = 0; sg < NW; sg++) {
-                        const int n = segc[sg];
-                        for (int base = 0; base < n; base += 32) {
-                            const int j = base + lane;
-                            bool pass = false;
-                            if (j < n) {
-                                const float4 c = sm.cpos[sg * SEG + j];
-                                const float dx = c.x - xo, dy = c.y - yo, dz = c.z - zo;
-                                pass = dx * dx + dy * dy + dz * dz < R2;
+                        for (int h = 0; h < 2; h++) {
+                            const int f = base + 32 * h + lane;
+                            pa[h] = pb[h] = false;
+                            sl[h] = 0;
+                            if (f < stot) {
+                                int o = segoff[0];
+#pragma unroll
+                                for (int i = 1; i < NW; i++)
+                                    if (f >= segp[i]) o = segoff[i];
+                                sl[h] = f - o;
+                                const float4 c = sm.cpos[sl[h]];
+                                float dx = c.x - qa.x, dy = c.y - qa.y, dz = c.z - qa.z;
+                                pa[h] = dx * dx + dy * dy + dz * dz < R2a;
+                                dx = c.x - qb.x;
+                                dy = c.y - qb.y;
+                                dz = c.z - qb.z;
+                                pb[h] = dx * dx + dy * dy + dz * dz < R2b;
                             }
-                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
-                            const int pos = cnt + __popc(bal & lt);
-                            if (pass && pos < LW) sm.wlist[w][pos] = (unsigned short)(sg * SEG + j);
-                            cnt += __popc(bal);
+                        }
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const unsigned ba = __ballot_sync(0xffffffffu, pa[h]);
+                            const unsigned bb = __ballot_sync(0xffffffffu, pb[h]);
+                            const int pa_ = ca + __popc(ba & lt), pb_ = cb + __popc(bb & lt);
+                            if (pa[h] && pa_ < LW) sm.wlist[w][0][pa_] = (unsigned short)sl[h];
+                            if (pb[h] && pb_ < LW) sm.wlist[w][1][pb_] = (unsigned short)sl[h];
+                            ca += __popc(ba);
+                            cb += __popc(bb);
                         }
                     }
-                    if (cnt > LW) {
+                    if (ca > LW || cb > LW) {
                         if (lane == 0) sm.overflow = 1;
-                        cnt = LW;
+                        ca = ca < LW ? ca : LW;
+                        cb = cb < LW ? cb : LW;
                     }
                     __syncwarp();
-                    const float uox = sm.aux[k], uoy = sm.auy[k], uoz = sm.auz[k];
-                    const float xn = sm.bx[k], yn = sm.by[k], zn = sm.bz[k];
-                    const float unx = sm.bux[k], uny = sm.buy[k], unz = sm.buz[k];
                     // FP64 lane sums: the 1e9 overlap clamp is exact in FP32 and
-                    // must cancel exactly between the old and the new sum
-                    for (int q = lane; q < cnt; q += 32) {
-                        const int j = sm.wlist[w][q];
+                    // must cancel exactly between the old and the new sum.  Entries
+                    // [0, ca) belong to particle a, [ca, ca + cb) to particle b.
+                    for (int q = lane; q < ca + cb; q += 32) {
+                        const bool isa = q < ca;
+                        const int j = isa ? sm.wlist[w][0][q] : sm.wlist[w][1][q - ca];
+                        const int k = isa ? ka : kb;
+                        const float4 P0 = sm.pst[k][0], P1 = sm.pst[k][1], P2 = sm.pst[k][2];
                         const float4 c = sm.cpos[j];
                         const float2 u = sm.cori[j];
-                        float dx = c.x - xo, dy = c.y - yo, dz = c.z - zo;
+                        float dx = c.x - P0.x, dy = c.y - P0.y, dz = c.z - P0.z;
                         float r2 = dx * dx + dy * dy + dz * dz;
-                        const float e0 = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, uox, uoy, uoz, c.w, u.x, u.y);
+                        const float e0 = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, P0.w, P1.x, P1.y, c.w, u.x, u.y);
                         const bool in0 = r2 < K.rc2;
-                        dx = c.x - xn;
-                        dy = c.y - yn;
-                        dz = c.z - zn;
+                        dx = c.x - P1.z;
+                        dy = c.y - P1.w;
+                        dz = c.z - P2.x;
                         r2 = dx * dx + dy * dy + dz * dz;
-                        const float e1 = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, unx, uny, unz, c.w, u.x, u.y);
+                        const float e1 = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, P2.y, P2.z, P2.w, c.w, u.x, u.y);
                         const bool in1 = r2 < K.rc2;
-                        so += in0 ? (double)e0 : 0.0;
-                        sn += in1 ? (double)e1 : 0.0;
+                        const double d0 = in0 ? (double)e0 : 0.0, d1 = in1 ? (double)e1 : 0.0;
+                        if (isa) {
+                            soa += d0;
+                            sna += d1;
+                        } else {
+                            sob += d0;
+                            snb += d1;
+                        }
                         np += (int)in0 + (int)in1;
                     }
                     __syncwarp();
                 }
 #pragma unroll
                 for (int o = 16; o >= 1; o >>= 1) {
-                    so += __shfl_xor_sync(0xffffffffu, so, o);
-                    sn += __shfl_xor_sync(0xffffffffu, sn, o);
+                    soa += __shfl_xor_sync(0xffffffffu, soa, o);
+                    sna += __shfl_xor_sync(0xffffffffu, sna, o);
+                    sob += __shfl_xor_sync(0xffffffffu, sob, o);
+                    snb += __shfl_xor_sync(0xffffffffu, snb, o);
                     np += __shfl_xor_sync(0xffffffffu, np, o);
                 }
                 if (lane == 0) {
-                    sm.Sold[k] = so;
-                    sm.Snew[k] = sn;
+                    sm.Sold[ka] = soa;
+                    sm.Snew[ka] = sna;
+                    if (has_b) {
+                        sm.Sold[kb] = sob;
+                        sm.Snew[kb] = snb;
+                    }
                 }
                 npairs += (unsigned long long)np;
             } else {
-                const int idx = (task - na) * 32 + lane;
+                const int idx = (task - nptask) * 32 + lane;
                 int npin = 0;
                 if (idx < npair) {
                     int q = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)idx)) * 0.5f);
@@ -363,35 +432,34 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
                     while ((q + 1) * q / 2 <= idx) q++;
                     const int pp = idx - q * (q - 1) / 2;
                     float A, B, Cc, D;
+                    const float4 Q0 = sm.pst[q][0], Q1 = sm.pst[q][1], Q2 = sm.pst[q][2];
+                    const float4 R0 = sm.pst[pp][0], R1 = sm.pst[pp][1], R2 = sm.pst[pp][2];
+                    // a(.) = (X0.x, X0.y, X0.z), u_a = (X0.w, X1.x, X1.y); b(.) = (X1.z, X1.w, X2.x), u_b = (X2.y, X2.z, X2.w)
                     {
-                        float dx = sm.ax[q] - sm.ax[pp], dy = sm.ay[q] - sm.ay[pp], dz = sm.az[q] - sm.az[pp];
+                        float dx = Q0.x - R0.x, dy = Q0.y - R0.y, dz = Q0.z - R0.z;
                         float r2 = dx * dx + dy * dy + dz * dz;
-                        A = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, sm.aux[pp], sm.auy[pp], sm.auz[pp], sm.aux[q],
-                                                sm.auy[q], sm.auz[q]);
+                        A = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, R0.w, R1.x, R1.y, Q0.w, Q1.x, Q1.y);
                         A = r2 < K.rc2 ? A : 0.0f;
                         npin += 2 * (r2 < K.rc2);
                     }
                     {
-                        float dx = sm.bx[q] - sm.ax[pp], dy = sm.by[q] - sm.ay[pp], dz = sm.bz[q] - sm.az[pp];
+                        float dx = Q1.z - R0.x, dy = Q1.w - R0.y, dz = Q2.x - R0.z;
                         float r2 = dx * dx + dy * dy + dz * dz;
-                        B = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, sm.aux[pp], sm.auy[pp], sm.auz[pp], sm.bux[q],
-                                                sm.buy[q], sm.buz[q]);
+                        B = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, R0.w, R1.x, R1.y, Q2.y, Q2.z, Q2.w);
                         B = r2 < K.rc2 ? B : 0.0f;
                         npin += (r2 < K.rc2);
                     }
                     {
-                        float dx = sm.ax[q] - sm.bx[pp], dy = sm.ay[q] - sm.by[pp], dz = sm.az[q] - sm.bz[pp];
+                        float dx = Q0.x - R1.z, dy = Q0.y - R1.w, dz = Q0.z - R2.x;
                         float r2 = dx * dx + dy * dy + dz * dz;
-                        Cc = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, sm.bux[pp], sm.buy[pp], sm.buz[pp], sm.aux[q],
-                                                 sm.auy[q], sm.auz[q]);
+                        Cc = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, R2.y, R2.z, R2.w, Q0.w, Q1.x, Q1.y);
                         Cc = r2 < K.rc2 ? Cc : 0.0f;
                         npin += (r2 < K.rc2);
                     }
                     {
-                        float dx = sm.bx[q] - sm.bx[pp], dy = sm.by[q] - sm.by[pp], dz = sm.bz[q] - sm.bz[pp];
+                        float dx = Q1.z - R1.z, dy = Q1.w - R1.w, dz = Q2.x - R2.x;
                         float r2 = dx * dx + dy * dy + dz * dz;
-                        D = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, sm.bux[pp], sm.buy[pp], sm.buz[pp], sm.bux[q],
-                                                sm.buy[q], sm.buz[q]);
+                        D = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, R2.y, R2.z, R2.w, Q2.y, Q2.z, Q2.w);
                         D = r2 < K.rc2 ? D : 0.0f;
                     }
                     // differences in FP64 (exact cancellation of the overlap clamp), then rounded
@@ -414,40 +482,51 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             continue;
         }
 
-        // ---- 5 warp per particle: in-cell row sums -> dE before the corrections ----
-        for (int k = w; k < na; k += NW) {
-            double s = 0.0;
-            for (int m = lane; m < na; m += 32) {
-                if (m < k) s += (double)sm.pBA[tri(m, k)];     // phi(n_k, o_m) - phi(o_k, o_m), k later
-                else if (m > k) s += (double)sm.pCA[tri(k, m)]; // k earlier in the pair
-            }
-#pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) sm.dEk[k] = (sm.Snew[k] - sm.Sold[k]) + s + v.tdU[g0 + k];
-        }
-        __syncthreads();
-
-        // ---- 6 sequential Metropolis scan (warp 0) ----
+        // ---- 5+6 warp 0: in-cell row sums (thread per particle) -> dE before the
+        //      corrections, then the sequential Metropolis scan in id order ----
         if (w == 0) {
-            double e0 = lane < na ? sm.dEk[lane] : 0.0;
-            double e1 = lane + 32 < na ? sm.dEk[lane + 32] : 0.0;
-            const double lu0 = lane < na ? v.tlu[g0 + lane] : 0.0;
-            const double lu1 = lane + 32 < na ? v.tlu[g0 + lane + 32] : 0.0;
+            double e0 = 0.0, e1 = 0.0;
+            for (int h = 0; h < 2; h++) {
+                const int k = lane + 32 * h;
+                if (k >= na) break;
+                // two partial sums per loop: independent FP64 add chains
+                double sa = 0.0, sb = 0.0, sc = 0.0, sd = 0.0;
+                const int kb = tri(0, k);
+                int m = 0;
+                for (; m + 1 < k; m += 2) { // phi(n_k, o_m) - phi(o_k, o_m), k later in the pair
+                    sa += (double)sm.pBA[kb + m];
+                    sb += (double)sm.pBA[kb + m + 1];
+                }
+                if (m < k) sa += (double)sm.pBA[kb + m];
+                m = k + 1;
+                for (; m + 1 < na; m += 2) { // k earlier in the pair
+                    sc += (double)sm.pCA[tri(k, m)];
+                    sd += (double)sm.pCA[tri(k, m + 1)];
+                }
+                if (m < na) sc += (double)sm.pCA[tri(k, m)];
+                const double s = (sa + sb) + (sc + sd);
+                const double d = (sm.Snew[k] - sm.Sold[k]) + s + sm.tdU[k];
+                if (h == 0) e0 = d;
+                else e1 = d;
+            }
             const double beta = p.k.beta;
             double dsum = 0.0;
             int nacc = 0, nhard = 0;
             for (int m = 0; m < na; m++) {
                 const int own = m & 31;
+                // this step's corrections and draws do not depend on the decision chain
+                const double c0 = (lane > m && lane < na) ? (double)sm.pcm[tri(m, lane)] : 0.0;
+                const double c1 = (lane + 32 > m && lane + 32 < na) ? (double)sm.pcm[tri(m, lane + 32)] : 0.0;
+                const double lum = sm.tlu[m];
+                const int hd = sm.hard[m];
                 const double val = __shfl_sync(0xffffffffu, m < 32 ? e0 : e1, own);
-                const double lum = __shfl_sync(0xffffffffu, m < 32 ? lu0 : lu1, own);
-                const int hd = sm.rad2[m] < 0.0f;
                 const bool acc = !hd && ((val <= 0.0) || (lum <= -beta * val));
                 nhard += hd;
                 if (acc) {
                     dsum += val;
                     nacc++;
-                    if (lane > m && lane < na) e0 += (double)sm.pcm[tri(m, lane)];
-                    if (lane + 32 > m && lane + 32 < na) e1 += (double)sm.pcm[tri(m, lane + 32)];
+                    e0 += c0;
+                    e1 += c1;
                 }
                 if (lane == 0) sm.acc[m] = acc;
             }
@@ -467,14 +546,14 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             const int g = g0 + k;
             const int acc = sm.acc[k];
             if (acc) {
-                v.px[g] = v.tnx[g];
-                v.py[g] = v.tny[g];
-                v.pz[g] = v.tnz[g];
-                v.ox[g] = v.tux[g];
-                v.oy[g] = v.tuy[g];
-                v.oz[g] = v.tuz[g];
+                v.px[g] = sm.tn[0][k];
+                v.py[g] = sm.tn[1][k];
+                v.pz[g] = sm.tn[2][k];
+                v.ox[g] = sm.tn[3][k];
+                v.oy[g] = sm.tn[4][k];
+                v.oz[g] = sm.tn[5][k];
             }
-            v.outcome[p.p_off + v.id[g]] = v.thard[g] ? 2 : acc;
+            v.outcome[p.p_off + sm.pid[k]] = sm.hard[k] ? 2 : acc;
         }
         __syncthreads();
     }
