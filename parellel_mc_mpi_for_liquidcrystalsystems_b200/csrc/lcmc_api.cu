@@ -51,6 +51,8 @@ struct lcmc_ctx {
     double *d_trial_d[8] = {nullptr}; // tnx tny tnz tux tuy tuz tdU tlu
     float *d_trial_f[3] = {nullptr};  // tdx tdy tdz
     unsigned char *d_thard = nullptr;
+    float4 *d_cl4 = nullptr;
+    float2 *d_cl2 = nullptr;
     // surrogate, recordings
     unsigned long long *d_feat_acc = nullptr;
     float *d_feat_f = nullptr;
@@ -445,6 +447,8 @@ static DevView view(const lcmc_ctx *c, int parity)
     v.tdy = c->d_trial_f[1];
     v.tdz = c->d_trial_f[2];
     v.thard = c->d_thard;
+    v.cl4 = c->d_cl4;
+    v.cl2 = c->d_cl2;
     v.feat_acc = c->d_feat_acc;
     v.feat_f = c->d_feat_f;
     v.rec_cap = c->rec_cap;
@@ -474,6 +478,8 @@ static void free_ctx(lcmc_ctx *c)
     for (int k = 0; k < 3; k++)
         if (c->d_trial_f[k]) cudaFree(c->d_trial_f[k]);
     if (c->d_thard) cudaFree(c->d_thard);
+    if (c->d_cl4) cudaFree(c->d_cl4);
+    if (c->d_cl2) cudaFree(c->d_cl2);
     void *more[] = {c->d_feat_acc, c->d_feat_f, c->d_rec_count, c->d_rec_x, c->d_rec_y, c->d_hist};
     for (void *p : more)
         if (p) cudaFree(p);
@@ -641,6 +647,8 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     for (int k = 0; k < 8; k++) ALLOC(c->d_trial_d[k], c->ntot);
     for (int k = 0; k < 3; k++) ALLOC(c->d_trial_f[k], c->ntot);
     ALLOC(c->d_thard, c->ntot);
+    ALLOC(c->d_cl4, c->ntot);
+    ALLOC(c->d_cl2, c->ntot);
     ALLOC(c->d_feat_acc, (size_t)n * 512 * 7);
     ALLOC(c->d_feat_f, (size_t)n * LCMC_FEAT);
 #undef ALLOC

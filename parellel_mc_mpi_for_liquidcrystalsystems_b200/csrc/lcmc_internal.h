@@ -97,6 +97,11 @@ struct DevView {
     double *tlu;               // log of the Metropolis draw
     float *tdx, *tdy, *tdz;    // displacement
     unsigned char *thard;      // 1 = colloid hard-core reject
+    // FP32 copy of the state of FP32-kernel systems, relative to each particle's
+    // own cell origin: (x, y, z, ux) and (uy, uz), unit orientation; written by
+    // the gather, kept current by the phase write-back
+    float4 *cl4;
+    float2 *cl2;
     // surrogate features and recordings
     unsigned long long *feat_acc; // [R x 512 x 7] pooled sums, fixed point 2^-32
     float *feat_f;             // [R x LCMC_FEAT] features of the current configuration

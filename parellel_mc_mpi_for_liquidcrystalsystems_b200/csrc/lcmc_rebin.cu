@@ -255,11 +255,18 @@ __global__ void k_gather(DevView v)
         v.tdU[g] = dU;
         v.tlu[g] = log_unit(u);
         v.thard[g] = (unsigned char)!ok;
+        // FP32 copy relative to the particle's own cell origin
+        const int cl = v.cid[src] - p.cell_off;
+        const int cx = cl % p.nc[0], cy = (cl / p.nc[0]) % p.nc[1], cz = cl / (p.nc[0] * p.nc[1]);
+        const double lx = fold_rel(ro[0], p.shift[0] + (double)cx * p.w[0], 0.5 * p.w[0], p.L[0], 1.0 / p.L[0]);
+        const double ly = fold_rel(ro[1], p.shift[1] + (double)cy * p.w[1], 0.5 * p.w[1], p.L[1], 1.0 / p.L[1]);
+        const double lz = fold_rel(ro[2], p.shift[2] + (double)cz * p.w[2], 0.5 * p.w[2], p.L[2], 1.0 / p.L[2]);
+        const double in = 1.0 / sqrt(eo[0] * eo[0] + eo[1] * eo[1] + eo[2] * eo[2]);
+        v.cl4[g] = make_float4((float)lx, (float)ly, (float)lz, (float)(eo[0] * in));
+        v.cl2[g] = make_float2((float)(eo[1] * in), (float)(eo[2] * in));
     }
 }
 
-// Block per replica: deterministic sums of the per-cell sweep results
-// (accepted dE, accepted count, hard-core rejects, pair/candidate counters).
 // Per-cell results of a sweep in chunks of LCMC_RED_CHUNK cells (blocks:
 // chunk, replica): dE, accepted, hard-core rejections, in-cutoff pairs and
 // stencil candidates (counts are exact in FP64).

@@ -23,9 +23,12 @@
 //   2 active   phase-start state and precomputed trial of each particle of the
 //              cell, coordinates relative to the cell origin (FP32)
 //   3 staging  the 26 static cells -> shared memory (float4 x,y,z,ux + float2
-//              uy,uz), folded across the periodic seam, pruned to the cell box
-//              grown by rc + max_displacement/2; warp w compacts its quarter of
-//              the candidates into its own segment (no block barrier per round)
+//              uy,uz), read from the FP32 copy of the state (coordinates
+//              relative to each particle's own cell origin, folded across the
+//              periodic seam by the gather) plus the stencil offset, pruned to
+//              the cell box grown by rc + max_displacement/2; warp w compacts its
+//              quarter of the candidates into its own segment (no block barrier
+//              per round)
 //   4 tasks    warps take tasks from a shared queue:
 //              particle task (two particles k, k + 1): cutoff test of every
 //                staged candidate, loaded once, against both old positions
@@ -59,18 +62,6 @@ __device__ __forceinline__ int find_replica_f(const int *off, int R, int a)
 }
 
 __device__ __forceinline__ int tri(int p, int q) { return (q * (q - 1)) / 2 + p; } // p < q
-
-// Coordinate relative to the active cell's origin o, folded by whole periods
-// into the window of the stencil cell it belongs to (centre cexp = (d + 1/2) w
-// for stencil offset d).  A stored coordinate may lie on either side of the
-// shifted periodic seam (cells that straddle it, or particles that crossed it
-// earlier in the sweep); the fold is exact because every particle stays within
-// w/2 + max_displacement/2 of its cell centre and w <= L/4.
-__device__ __forceinline__ double fold_rel(double x, double o, double cexp, double L, double invL)
-{
-    const double r = x - o;
-    return r - L * rint((r - cexp) * invL);
-}
 
 template <int NT, int AMAX, int SEG, int LW>
 struct FastSmem {
@@ -153,11 +144,6 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
         const int cz = 2 * (loc / nay) + ((col >> 2) & 1);
         const int cell = p.cell_off + (cz * nc1 + cy) * nc0 + cx;
         const double w0 = p.w[0], w1 = p.w[1], w2 = p.w[2];
-        const double L0 = p.L[0], L1 = p.L[1], L2 = p.L[2];
-        const double iL0 = 1.0 / L0, iL1 = 1.0 / L1, iL2 = 1.0 / L2;
-        const double o0 = p.shift[0] + (double)cx * w0;
-        const double o1 = p.shift[1] + (double)cy * w1;
-        const double o2 = p.shift[2] + (double)cz * w2;
         const FastK K = fast_consts(p.k);
 
         // ---- 1 stencil ----
@@ -203,16 +189,12 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
         const float rcf = (float)p.k.rc;
         for (int k = t; k < na; k += NT) {
             const int g = g0 + k;
-            const double qx = fold_rel(v.px[g], o0, 0.5 * w0, L0, iL0);
-            const double qy = fold_rel(v.py[g], o1, 0.5 * w1, L1, iL1);
-            const double qz = fold_rel(v.pz[g], o2, 0.5 * w2, L2, iL2);
-            const double ex = v.ox[g], ey = v.oy[g], ez = v.oz[g];
-            const float en = rsqrtf((float)(ex * ex + ey * ey + ez * ez));
+            const float4 c4 = v.cl4[g]; // relative to this cell's origin
+            const float2 c2 = v.cl2[g];
             const float dx = v.tdx[g], dy = v.tdy[g], dz = v.tdz[g];
-            const float ax = (float)qx, ay = (float)qy, az = (float)qz;
-            sm.pst[k][0] = make_float4(ax, ay, az, (float)ex * en);
-            sm.pst[k][1] = make_float4((float)ey * en, (float)ez * en, ax + dx, ay + dy);
-            sm.pst[k][2] = make_float4(az + dz, (float)v.tux[g], (float)v.tuy[g], (float)v.tuz[g]);
+            sm.pst[k][0] = c4;
+            sm.pst[k][1] = make_float4(c2.x, c2.y, c4.x + dx, c4.y + dy);
+            sm.pst[k][2] = make_float4(c4.z + dz, (float)v.tux[g], (float)v.tuy[g], (float)v.tuz[g]);
             const float rr = rcf + sqrtf(dx * dx + dy * dy + dz * dz) + 1e-3f;
             const unsigned char hd = v.thard[g];
             sm.rad2[k] = hd ? -1.0f : rr * rr;
@@ -256,20 +238,19 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
                             else hi = mid;
                         }
                         const int g = sm.st_start[sl] + (f - sm.st_pre[sl]);
-                        const double gx = v.px[g], gy = v.py[g], gz = v.pz[g];
-                        const double ex = v.ox[g], ey = v.oy[g], ez = v.oz[g];
-                        // stencil offset of slot sl is (sl % 3, sl / 3 % 3, sl / 9) - 1
-                        x[h] = (float)fold_rel(gx, o0, ((double)(sl % 3) - 0.5) * w0, L0, iL0);
-                        y[h] = (float)fold_rel(gy, o1, ((double)((sl / 3) % 3) - 0.5) * w1, L1, iL1);
-                        z[h] = (float)fold_rel(gz, o2, ((double)(sl / 9) - 0.5) * w2, L2, iL2);
+                        const float4 c4 = v.cl4[g]; // relative to its own cell's origin
+                        const float2 c2 = v.cl2[g];
+                        // stencil offset of slot sl is (sl % 3, sl / 3 % 3, sl / 9) - 1 cells
+                        x[h] = c4.x + (float)(sl % 3 - 1) * wx;
+                        y[h] = c4.y + (float)((sl / 3) % 3 - 1) * wy;
+                        z[h] = c4.z + (float)(sl / 9 - 1) * wz;
                         const float qx = fmaxf(fmaxf(-hb - x[h], x[h] - (wx + hb)), 0.0f);
                         const float qy = fmaxf(fmaxf(-hb - y[h], y[h] - (wy + hb)), 0.0f);
                         const float qz = fmaxf(fmaxf(-hb - z[h], z[h] - (wz + hb)), 0.0f);
                         keep[h] = qx * qx + qy * qy + qz * qz < prune2;
-                        const float in = rsqrtf((float)(ex * ex + ey * ey + ez * ez));
-                        ux[h] = (float)ex * in;
-                        uy[h] = (float)ey * in;
-                        uz[h] = (float)ez * in;
+                        ux[h] = c4.w;
+                        uy[h] = c2.x;
+                        uz[h] = c2.y;
                     }
                 }
 #pragma unroll
@@ -552,6 +533,9 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
                 v.ox[g] = sm.tn[3][k];
                 v.oy[g] = sm.tn[4][k];
                 v.oz[g] = sm.tn[5][k];
+                const float4 P1 = sm.pst[k][1], P2 = sm.pst[k][2];
+                v.cl4[g] = make_float4(P1.z, P1.w, P2.x, P2.y);
+                v.cl2[g] = make_float2(P2.z, P2.w);
             }
             v.outcome[p.p_off + sm.pid[k]] = sm.hard[k] ? 2 : acc;
         }

@@ -6,6 +6,18 @@
 
 namespace lcmc {
 
+// Coordinate relative to a cell origin o, folded by whole periods into the
+// window of the stencil cell it belongs to (centre cexp = (d + 1/2) w
+// for stencil offset d).  A stored coordinate may lie on either side of the
+// shifted periodic seam (cells that straddle it, or particles that crossed it
+// earlier in the sweep); the fold is exact because every particle stays within
+// w/2 + max_displacement/2 of its cell centre and w <= L/4.
+__device__ __forceinline__ double fold_rel(double x, double o, double cexp, double L, double invL)
+{
+    const double r = x - o;
+    return r - L * rint((r - cexp) * invL);
+}
+
 // apply_pbc (MCnptColloid.c:2420-2430): a single +-L fold per axis.
 __device__ __forceinline__ void apply_pbc(double r[3], const double L[3])
 {
