@@ -346,7 +346,7 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
         "seconds_total": time.perf_counter() - t_start}
 
 
-def npt_workload(lcmc, torch, n, steps, warmup):
+def npt_workload(lcmc, torch, n, steps, warmup, screen=False):
     """NPT sweeps of one system (colloid R = 8, T* = 0.85, P* = 2): a dilute
     start compressed for 700 sweeps (dlnV_max 0.05), `warmup` sweeps at
     dlnV_max = 0.01, then `steps` timed sweeps; device time per sweep by part."""
@@ -358,6 +358,7 @@ def npt_workload(lcmc, torch, n, steps, warmup):
         st, box = s.download()
     with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01)) as s:
         s.upload(*st, box)
+        s.set_fp32_screen(screen)
         s.sweep(max(3, warmup))
         parts, total = [], 0.0
         for _ in range(steps):
@@ -370,6 +371,8 @@ def npt_workload(lcmc, torch, n, steps, warmup):
                 "steps": steps, "ms_per_sweep": 1e3 * total / steps,
                 "ms_parts_median": {"rebin": parts[0], "colour_phases": parts[1], "volume_move": parts[2],
                                     "finalize": parts[3]},
+                "fp32_screen": screen, "volume_accepted": stt["volume_accepted"],
+                "volume_stage1_rejected": stt["volume_stage1_rejected"],
                 "rho": n / float(np.prod(stt["box"])), "energy_per_particle": stt["energy"] / n,
                 "kernels_per_sweep": s.kernels_per_sweep()}
 
@@ -389,6 +392,7 @@ def main():
     ap.add_argument("--workload", default="moves", choices=["moves", "npt"],
                     help="npt: time NPT sweeps of one compressed system (per-part device times) instead")
     ap.add_argument("--npt-n", type=int, default=262144)
+    ap.add_argument("--npt-screen", action="store_true", help="npt workload with the FP32-pair volume screen")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -420,7 +424,7 @@ def main():
     torch.cuda.set_device(local)
     if args.workload == "npt":
         if rank == 0:
-            print(json.dumps(npt_workload(lcmc, torch, args.npt_n, args.steps, args.warmup)))
+            print(json.dumps(npt_workload(lcmc, torch, args.npt_n, args.steps, args.warmup, args.npt_screen)))
         return 0
     dist = None
     if world > 1:

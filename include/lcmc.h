@@ -227,6 +227,17 @@ int lcmc_gemm_bf16(const float *A, const float *B, float *C, int M, int N, int K
  * output to dU / (N delta).  m = NULL switches it off.  The network must stay
  * alive while set. */
 int lcmc_set_surrogate(lcmc_ctx *ctx, lcmc_mlp *m, double target_scale);
+/* Delayed-acceptance volume moves whose stage 1 tests the energy change
+ * evaluated with FP32 pair terms (FP64 sums; the same in-cutoff pairs as the
+ * FP64 recompute, each pair term a function of the two particles' FP64
+ * coordinates, so the screen is odd under x <-> y), with the plain move's
+ * random draw; stage 2 tests exp(-beta (dU - dU~)) with the exact FP64 dU.
+ * |dU - dU~| is about 1e-3 kT, so the two stages decide as the plain move
+ * does, but the FP64 recompute runs only for moves that pass stage 1.  NPT
+ * replicas on the FP32 kernel only; on = 0 switches it off.  Setting it
+ * clears the learned surrogate, and lcmc_set_surrogate clears it.  No
+ * counterpart in the reference (it has no volume move). */
+int lcmc_set_fp32_screen(lcmc_ctx *ctx, int on);
 #define LCMC_FEATURES 4097
 /* Record (features of x, exact dU / (N delta)) of every exactly evaluated
  * volume move (capacity samples; 0 stops and frees); fetch them (x: n x 4097). */

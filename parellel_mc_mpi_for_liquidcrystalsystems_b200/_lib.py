@@ -94,6 +94,7 @@ EXPORTS = {
     "lcmc_mlp_set_params": ([C.c_void_p, FP], C.c_int),
     "lcmc_gemm_bf16": ([FP, FP, FP, C.c_int, C.c_int, C.c_int], C.c_int),
     "lcmc_set_surrogate": ([C.c_void_p, C.c_void_p, C.c_double], C.c_int),
+    "lcmc_set_fp32_screen": ([C.c_void_p, C.c_int], C.c_int),
     "lcmc_record_volume_samples": ([C.c_void_p, C.c_int], C.c_int),
     "lcmc_get_volume_samples": ([C.c_void_p, FP, FP, C.c_int], C.c_int),
     "lcmc_record_history": ([C.c_void_p, C.c_int], C.c_int),

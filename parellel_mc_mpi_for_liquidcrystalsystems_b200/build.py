@@ -33,6 +33,7 @@ SOURCES = {
     "lcmc_noalloc.cu": ["-fmad=false"],
     "lcmc_mlp.cu": [],
     "lcmc_da.cu": [],
+    "lcmc_screen.cu": ["-fmad=false"],  # forms the scaled vectors exactly as the volume scaling does
 }
 
 

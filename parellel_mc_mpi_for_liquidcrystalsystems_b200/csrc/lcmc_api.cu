@@ -62,14 +62,15 @@ struct lcmc_ctx {
     int hist_cap = 0;
     double *d_hist = nullptr;
     lcmc_mlp *mlp = nullptr;
-    bool any_da = false;
+    bool any_da = false;     // an NPT replica uses the learned surrogate
+    bool any_screen = false; // an NPT replica uses the FP32-pair screen
     int cur = 0;
     bool uploaded_all = false;
     std::vector<char> uploaded;
     // kernels
     int kernel_override = -1;
     int fast_variant = 0;
-    int grid_elem = 0, grid_exact = 0, grid_fast = 0, grid_energy = 0;
+    int grid_elem = 0, grid_exact = 0, grid_fast = 0, grid_energy = 0, grid_screen = 0;
     bool any_fast = false, any_exact = false, any_npt = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -671,6 +672,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     c->grid_elem = 4 * c->sms;
     c->grid_exact = 4 * c->sms;
     c->grid_energy = energy_exact_blocks_per_sm() * c->sms;
+    c->grid_screen = screen_blocks_per_sm() * c->sms;
     c->grid_fast = fast_blocks_per_sm(c->fast_variant) * c->sms;
     int rc = upload_replica_table(c);
     if (rc) {
@@ -741,6 +743,7 @@ static void enqueue_sweep(lcmc_ctx *c, int parity)
         if (c->any_da || c->rec_cap > 0)
             launch_features(v, c->stream, c->any_da ? mlp_input(c->mlp) : nullptr, c->any_da ? mlp_ld(c->mlp) : 0,
                             c->grid_elem);
+        if (c->any_screen) launch_screen(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_screen, c->fast_variant & 1);
         if (c->any_da) {
             const int B = (2 * c->R + 127) / 128 * 128;
             const float *y = mlp_forward_device(c->mlp, B, c->stream);
@@ -858,6 +861,7 @@ extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
     int n = 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 2;
     if (ctx->any_npt && (ctx->any_da || ctx->rec_cap > 0)) n += 2;
     if (ctx->any_npt && ctx->any_da) n += 6;
+    if (ctx->any_npt && ctx->any_screen) n += 3; // screen energies, chunk sums, stage 1
     if (ctx->any_npt && ctx->rec_cap > 0) n += 1;
     if (ctx->hist_cap > 0) n += 2;
     return n;
@@ -868,6 +872,8 @@ static int push_replica_fields(lcmc_ctx *c, int r)
     Replica &rp = c->rep[r];
     char *base = (char *)c->d_rep + sizeof(Replica) * r;
     CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, da_on), &rp.da_on, sizeof(int), cudaMemcpyHostToDevice,
+                                c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, da_kind), &rp.da_kind, sizeof(int), cudaMemcpyHostToDevice,
                                 c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, da_scale), &rp.da_scale, sizeof(double),
                                 cudaMemcpyHostToDevice, c->stream));
@@ -882,11 +888,31 @@ extern "C" int lcmc_set_surrogate(lcmc_ctx *ctx, lcmc_mlp *m, double target_scal
         return set_err(ctx, LCMC_EINVAL, "surrogate needs 4097 inputs and a batch of at least 2 x replicas");
     ctx->mlp = m;
     ctx->any_da = false;
+    ctx->any_screen = false; // one screen at a time
     for (int r = 0; r < ctx->R; r++) {
         Replica &rp = ctx->rep[r];
         rp.da_on = (m && rp.ensemble == 2) ? 1 : 0;
+        rp.da_kind = rp.da_on ? 1 : 0;
         rp.da_scale = target_scale;
         ctx->any_da = ctx->any_da || rp.da_on;
+        int rc = push_replica_fields(ctx, r);
+        if (rc) return rc;
+    }
+    invalidate_graphs(ctx);
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_set_fp32_screen(lcmc_ctx *ctx, int on)
+{
+    if (!ctx) return LCMC_EINVAL;
+    ctx->mlp = nullptr; // one screen at a time
+    ctx->any_da = false;
+    ctx->any_screen = false;
+    for (int r = 0; r < ctx->R; r++) {
+        Replica &rp = ctx->rep[r];
+        rp.da_on = (on && rp.ensemble == 2 && rp.kernel == 1) ? 1 : 0;
+        rp.da_kind = rp.da_on ? 2 : 0;
+        ctx->any_screen = ctx->any_screen || rp.da_on;
         int rc = push_replica_fields(ctx, r);
         if (rc) return rc;
     }

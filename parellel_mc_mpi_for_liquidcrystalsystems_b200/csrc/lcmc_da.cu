@@ -50,7 +50,7 @@ __global__ void k_feat_accum(DevView v)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.ntot; i += gridDim.x * blockDim.x) {
         const int r = v.p2r[i];
         const Replica &p = v.rep[r];
-        if (p.ensemble != 2 || !(p.da_on || v.rec_cap > 0)) continue;
+        if (p.ensemble != 2 || !(p.da_kind == 1 || v.rec_cap > 0)) continue;
         int c3[3];
         const double pos[3] = {v.px[i], v.py[i], v.pz[i]};
         double d[3], dd = 0.0;
@@ -84,7 +84,7 @@ __global__ void k_feat_finalize(DevView v, __nv_bfloat16 *X, int ldx)
 {
     const int r = blockIdx.x;
     const Replica &p = v.rep[r];
-    if (p.ensemble != 2 || !(p.da_on || v.rec_cap > 0)) return;
+    if (p.ensemble != 2 || !(p.da_kind == 1 || v.rec_cap > 0)) return;
     const double V = p.L[0] * p.L[1] * p.L[2];
     const double inv_vc = (double)FC / V / 0.3;
     // The y row is what these kernels compute for the scaled configuration
@@ -136,18 +136,14 @@ __global__ void k_da_stage1(DevView v, const float *y)
 {
     for (int r = threadIdx.x; r < v.R; r += blockDim.x) {
         Replica &p = v.rep[r];
-        if (p.ensemble != 2) continue;
-        if (!p.da_on) {
-            p.vol_stage1 = 1;
-            continue;
-        }
+        if (p.ensemble != 2 || !p.da_on || p.da_kind != 1) continue;
         const double dUs = (double)p.n * p.da_scale * p.vol_delta * 0.5 * ((double)y[2 * r] + (double)y[2 * r + 1]);
         const double V = p.L[0] * p.L[1] * p.L[2];
         const double dV = V * expm1_small(p.vol_delta);
         const double lnA1 = -p.k.beta * (dUs + p.pressure * dV) + (double)(p.n + 1) * p.vol_delta;
         U4 o = draw(p.key, SWEEP_ID, p.sweep, TAG_VOLUME);
         p.vol_dU_sur = dUs;
-        p.vol_stage1 = (lnA1 >= 0.0 || log_unit(u01(o.z)) <= lnA1) ? 1 : 0;
+        p.vol_stage1 = (lnA1 >= 0.0 || log_unit(u01(o.z)) <= lnA1) ? 2 : 0;
     }
 }
 
@@ -161,7 +157,7 @@ __global__ void k_record_samples(DevView v)
     int slot = *v.rec_count;
     for (int r = 0; r < v.R; r++) {
         const Replica &p = v.rep[r];
-        if (p.ensemble != 2 || p.vol_state == 3 || !p.vol_stage1) continue;
+        if (p.ensemble != 2 || p.vol_state == 3 || p.vol_stage1 == 0) continue;
         if (slot < v.rec_cap) {
             const float *src = v.feat_f + (size_t)r * LCMC_FEAT;
             float *dst = v.rec_x + (size_t)slot * LCMC_FEAT;

@@ -175,6 +175,26 @@ __device__ __forceinline__ float pair_fast_21(const FastK &k, float dx, float dy
     return dr < 0.001f ? 1.0e9f : v;
 }
 
+// FP32 constants of a system for the FP32 pair term.
+__device__ __forceinline__ FastK fast_consts(const GBConsts &k)
+{
+    FastK K;
+    K.rc2 = k.f_rc2;
+    K.chi = k.f_chi;
+    K.chi_sq = k.f_chi_sq;
+    K.chip = k.f_chip;
+    K.chip_sq = k.f_chip_sq;
+    K.sigma0 = k.f_sigma0;
+    K.four_eps0 = k.f_4eps0;
+    K.half_chi = k.f_half_chi;
+    K.half_chip = k.f_half_chip;
+    K.mu_code = k.mu_code;
+    K.nu_code = k.nu_code;
+    K.mu = (float)k.mu;
+    K.nu = (float)k.nu;
+    return K;
+}
+
 template <bool SPEC21>
 __device__ __forceinline__ float pair_fast_t(const FastK &k, float dx, float dy, float dz, float r2, float eix,
                                              float eiy, float eiz, float ejx, float ejy, float ejz);

@@ -39,8 +39,9 @@ struct Replica {
     double vol_delta, vol_lambda, vol_U_old, vol_U_new;
     int vol_state; // 0 none, 1 accepted, 2 rejected, 3 hard-core reject, 4 rejected by the surrogate (stage 1)
     // delayed acceptance with the learned surrogate
-    int da_on;
-    int vol_stage1;    // 1 = the exact stage runs this sweep
+    int da_on;         // a stage-1 screen is set for this replica
+    int da_kind;       // 1 the learned surrogate, 2 the FP32-pair energy change
+    int vol_stage1;    // this sweep: 0 rejected by the screen, 1 no screen, 2 passed the screen
     double da_scale;   // surrogate output -> dU / N
     double vol_dU_sur; // surrogate dU of this sweep's move
 };

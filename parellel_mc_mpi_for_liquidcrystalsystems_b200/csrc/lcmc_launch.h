@@ -26,6 +26,11 @@ int fast_blocks_per_sm(int variant);
 
 // lcmc_misc.cu
 void launch_q_chunk_sums(const DevView &v, cudaStream_t s); // Q-tensor chunk sums of every replica
+// chunk sums of (e0, e1, hard) of the NPT replicas not rejected at stage 1
+void launch_chunk_sums_volume(const DevView &v, cudaStream_t s, const double *e0, const double *e1, const int *hard);
+// FP32-pair screen of the volume move: energies at V and V', chunk sums, stage 1
+void launch_screen(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid, bool spec21);
+int screen_blocks_per_sm();
 void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, int replica_only);
 void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid);
 void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out);

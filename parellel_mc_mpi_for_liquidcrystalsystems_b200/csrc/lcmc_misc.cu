@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(256) k_chunk_sums(DevView v, const double *e0,
     const Replica &p = v.rep[r];
     const int i0 = c * LCMC_RED_CHUNK;
     if (i0 >= p.n) return;
-    if (MODE == 1 && (p.ensemble != 2 || (p.da_on && !p.vol_stage1))) return;
+    if (MODE == 1 && (p.ensemble != 2 || p.vol_stage1 == 0)) return;
     const int i1 = min(p.n, i0 + LCMC_RED_CHUNK);
     double s[K];
 #pragma unroll
@@ -86,7 +86,7 @@ __global__ void k_volume_propose(DevView v)
         U4 o = draw(p.key, SWEEP_ID, p.sweep, TAG_VOLUME);
         p.vol_delta = p.dlnv_max * (2.0 * u01(o.x) - 1.0);
         p.vol_lambda = 1.0 + expm1_small(p.vol_delta / 3.0);
-        p.vol_stage1 = 1; // the surrogate's stage 1 may clear it
+        p.vol_stage1 = 1; // a screen's stage 1 sets 0 (rejected) or 2 (passed)
         p.vol_dU_sur = 0.0;
     }
 }
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(256) k_volume_accept(DevView v)
     const int r = blockIdx.x;
     Replica &p = v.rep[r];
     if (p.ensemble != 2) return;
-    if (p.da_on && !p.vol_stage1) { // rejected by the surrogate: no exact energy was computed
+    if (p.vol_stage1 == 0) { // rejected by the screen: no exact energy was computed
         if (threadIdx.x == 0) {
             v.stats[r].vol_att += 1ull;
             v.stats[r].vol_s1rej += 1ull;
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256) k_volume_accept(DevView v)
         int state;
         if (H) {
             state = 3;
-        } else if (p.da_on) { // stage 2 of delayed acceptance: exact dU against the surrogate's
+        } else if (p.vol_stage1 == 2) { // stage 2 of delayed acceptance: exact dU against the screen's
             const double lnA2 = -p.k.beta * ((U1 - U0) - p.vol_dU_sur);
             U4 o = draw(p.key, SWEEP_ID, p.sweep, TAG_VOLUME);
             state = (lnA2 >= 0.0 || log_unit(u01(o.w)) <= lnA2) ? 1 : 2;
@@ -216,6 +216,11 @@ void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, in
     k_energy_reduce<<<v.R, 256, 0, s>>>(v, replica_only);
 }
 
+void launch_chunk_sums_volume(const DevView &v, cudaStream_t s, const double *e0, const double *e1, const int *hard)
+{
+    k_chunk_sums<3, 1><<<chunk_grid(v), 256, 0, s>>>(v, e0, e1, hard);
+}
+
 void launch_q_chunk_sums(const DevView &v, cudaStream_t s)
 {
     k_chunk_sums<6, 2><<<chunk_grid(v), 256, 0, s>>>(v, nullptr, nullptr, nullptr);
@@ -235,7 +240,7 @@ void launch_volume_propose(const DevView &v, cudaStream_t s) { k_volume_propose<
 void launch_volume_finish(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid)
 {
     launch_energy_exact(v, s, e0, e1, hard, 1, grid);
-    k_chunk_sums<3, 1><<<chunk_grid(v), 256, 0, s>>>(v, e0, e1, hard);
+    launch_chunk_sums_volume(v, s, e0, e1, hard);
     k_volume_accept<<<v.R, 256, 0, s>>>(v);
     if (v.rec_cap > 0) launch_record_samples(v, s);
     k_volume_scale<<<grid, 256, 0, s>>>(v);

@@ -261,9 +261,10 @@ __global__ void k_gather(DevView v)
         const double lx = fold_rel(ro[0], p.shift[0] + (double)cx * p.w[0], 0.5 * p.w[0], p.L[0], 1.0 / p.L[0]);
         const double ly = fold_rel(ro[1], p.shift[1] + (double)cy * p.w[1], 0.5 * p.w[1], p.L[1], 1.0 / p.L[1]);
         const double lz = fold_rel(ro[2], p.shift[2] + (double)cz * p.w[2], 0.5 * p.w[2], p.L[2], 1.0 / p.L[2]);
-        const double in = 1.0 / sqrt(eo[0] * eo[0] + eo[1] * eo[1] + eo[2] * eo[2]);
-        v.cl4[g] = make_float4((float)lx, (float)ly, (float)lz, (float)(eo[0] * in));
-        v.cl2[g] = make_float2((float)(eo[1] * in), (float)(eo[2] * in));
+        float ux, uy, uz;
+        unit_f32(eo[0], eo[1], eo[2], ux, uy, uz);
+        v.cl4[g] = make_float4((float)lx, (float)ly, (float)lz, ux);
+        v.cl2[g] = make_float2(uy, uz);
     }
 }
 

@@ -47,6 +47,7 @@
 #include "lcmc_gb.cuh"
 #include "lcmc_internal.h"
 #include "lcmc_rng.cuh"
+#include "lcmc_trial.cuh"
 
 namespace lcmc {
 
@@ -88,24 +89,6 @@ struct FastSmem {
     unsigned long long pairs;
 };
 
-__device__ __forceinline__ FastK fast_consts(const GBConsts &k)
-{
-    FastK K;
-    K.rc2 = k.f_rc2;
-    K.chi = k.f_chi;
-    K.chi_sq = k.f_chi_sq;
-    K.chip = k.f_chip;
-    K.chip_sq = k.f_chip_sq;
-    K.sigma0 = k.f_sigma0;
-    K.four_eps0 = k.f_4eps0;
-    K.half_chi = k.f_half_chi;
-    K.half_chip = k.f_half_chip;
-    K.mu_code = k.mu_code;
-    K.nu_code = k.nu_code;
-    K.mu = (float)k.mu;
-    K.nu = (float)k.nu;
-    return K;
-}
 
 __device__ __forceinline__ void cell_failed(const DevView &v, int r, int cell, int flag)
 {
@@ -194,7 +177,9 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             const float dx = v.tdx[g], dy = v.tdy[g], dz = v.tdz[g];
             sm.pst[k][0] = c4;
             sm.pst[k][1] = make_float4(c2.x, c2.y, c4.x + dx, c4.y + dy);
-            sm.pst[k][2] = make_float4(c4.z + dz, (float)v.tux[g], (float)v.tuy[g], (float)v.tuz[g]);
+            float tux, tuy, tuz; // the trial orientation as the FP32 state copy will hold it
+            unit_f32(v.tux[g], v.tuy[g], v.tuz[g], tux, tuy, tuz);
+            sm.pst[k][2] = make_float4(c4.z + dz, tux, tuy, tuz);
             const float rr = rcf + sqrtf(dx * dx + dy * dy + dz * dz) + 1e-3f;
             const unsigned char hd = v.thard[g];
             sm.rad2[k] = hd ? -1.0f : rr * rr;

@@ -18,6 +18,19 @@ __device__ __forceinline__ double fold_rel(double x, double o, double cexp, doub
     return r - L * rint((r - cexp) * invL);
 }
 
+// FP32 unit orientation of an FP64 orientation, with explicitly rounded FP64
+// operations (no contraction into FMA, whatever the file's flags), so every
+// kernel that forms it gets the same bits: the FP32 state copy written by the
+// gather and by the phase write-back, read by the FP32-pair volume screen.
+__device__ __forceinline__ void unit_f32(double x, double y, double z, float &ux, float &uy, float &uz)
+{
+    const double n2 = __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+    const double in = __ddiv_rn(1.0, __dsqrt_rn(n2));
+    ux = (float)__dmul_rn(x, in);
+    uy = (float)__dmul_rn(y, in);
+    uz = (float)__dmul_rn(z, in);
+}
+
 // apply_pbc (MCnptColloid.c:2420-2430): a single +-L fold per axis.
 __device__ __forceinline__ void apply_pbc(double r[3], const double L[3])
 {

@@ -159,6 +159,12 @@ class GBSystem:
             self._check(lib().lcmc_set_surrogate(self._h, surrogate.handle, surrogate.scale))
             self._surrogate = surrogate  # keep it alive while set
 
+    def set_fp32_screen(self, on=True):
+        """Delayed-acceptance volume moves screened by the FP32-pair energy
+        change (NPT replicas on the FP32 kernel); clears a surrogate."""
+        self._check(lib().lcmc_set_fp32_screen(self._h, int(bool(on))))
+        self._surrogate = None
+
     def record_volume_samples(self, capacity):
         """Record (features, exact dU / (N delta)) of the next `capacity` exactly
         evaluated volume moves (0 stops and frees)."""
