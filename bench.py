@@ -18,8 +18,8 @@ oracle/_ref with its OpenMP pragmas) on the host cores.
 
 The line also carries `npt_da`: effective samples per second of the P2 (and
 volume) series of NPT sweeps at N = 262,144 with a colloid (R = 8), plain
-volume moves against delayed acceptance with the learned surrogate
-(`--da-sweeps` per arm, 0 skips it).
+volume moves against delayed acceptance with the learned surrogate and with
+the FP32-pair screen (`--da-sweeps` per arm, 0 skips it).
 """
 import argparse
 import ctypes as C
@@ -299,19 +299,27 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
     k = min(4000, int(keep.sum()))
     corr = float(np.corrcoef(sur.predict(x[keep][:k]), y[keep][:k])[0, 1])
 
-    # the N = 262,144 system: compress from a dilute start, then both arms from one state
+    # the N = 262,144 system: compress from a dilute start, settle at dlnV_max
+    # 0.01, then every arm from that one state with one seed
     n = 262144
     with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05)) as s:
         st, box = dilute_start(n, 0.06, 8.0, 12)
         s.upload(*st, box)
         s.sweep(1000)
         st4, box4 = s.download()
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 13, 0.01)) as s:
+        s.upload(*st4, box4)
+        s.sweep(1000)
+        st4, box4 = s.download()
     arms = {}
-    for name, use in (("plain", False), ("delayed", True)):
+    for name in ("plain", "learned", "fp32_screen"):
         with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01)) as s:
             s.upload(*st4, box4)
-            s.set_surrogate(sur if use else None)
-            s.sweep(300)
+            if name == "learned":
+                s.set_surrogate(sur)
+            elif name == "fp32_screen":
+                s.set_fp32_screen(True)
+            s.sweep(100)
             st0 = s.stats()
             s.record_history(sweeps)
             secs = timed_sweeps(torch, s, sweeps)
@@ -325,24 +333,35 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
                 "volume_ess_per_s": sweeps / (2 * tv) / secs, "rho_mean": float(np.mean(n / V)),
                 "volume_accepted": st1["volume_accepted"] - st0["volume_accepted"],
                 "volume_stage1_rejected": st1["volume_stage1_rejected"] - st0["volume_stage1_rejected"],
+                "exact_volume_energies": (st1["volume_attempted"] - st0["volume_attempted"])
+                                         - (st1["volume_stage1_rejected"] - st0["volume_stage1_rejected"]),
                 "sweep_ms_parts": [round(float(t), 4) for t in s.last_sweep_timing()]}
+            if name == "plain":
+                p2_plain = p2
+            elif name == "fp32_screen":
+                arms[name]["p2_series_equals_plain"] = bool(np.array_equal(p2, p2_plain))
     sur.close()
-    pl, de = arms["plain"], arms["delayed"]
+    pl, le, sc = arms["plain"], arms["learned"], arms["fp32_screen"]
     return {
         "metric": "NPT P2 ESS/s, delayed-accept vs plain",
         "workload": "NPT N=262144, colloid R=8, T*=0.85, P*=2.0, dlnV_max=0.01 (one move per sweep), GB(3,5,2,1), "
                     "FP32 sweeps, FP64 volume energies; compressed for 1000 sweeps (dlnV_max 0.05) from a dilute "
-                    "lattice (rho 0.06), then 300 sweeps before each timed arm",
+                    "lattice (rho 0.06), 1000 sweeps at dlnV_max 0.01, then 100 sweeps before each timed arm; "
+                    "every arm from the same state and seed",
         "training": {"samples": int(len(y)), "used": int(keep.sum()), "replicas": nr, "n": n1, "colloid_R": 5.0,
                      "T": 0.9, "pressures": [pres[0], pres[-1]], "rho_range": [float(min(rho)), float(max(rho))],
                      "train_seconds": t_train, "final_loss": sur.history[-1] if sur.history else None,
                      "pred_corr": corr},
-        "plain": pl, "delayed": de,
-        "p2_ess_per_s_ratio": de["p2_ess_per_s"] / pl["p2_ess_per_s"],
-        "volume_ess_per_s_ratio": de["volume_ess_per_s"] / pl["volume_ess_per_s"],
-        "sweeps_per_s_ratio": pl["ms_per_sweep"] / de["ms_per_sweep"],
+        "plain": pl, "learned": le, "fp32_screen": sc,
+        "p2_ess_per_s_ratio": {"learned": le["p2_ess_per_s"] / pl["p2_ess_per_s"],
+                               "fp32_screen": sc["p2_ess_per_s"] / pl["p2_ess_per_s"]},
+        "volume_ess_per_s_ratio": {"learned": le["volume_ess_per_s"] / pl["volume_ess_per_s"],
+                                   "fp32_screen": sc["volume_ess_per_s"] / pl["volume_ess_per_s"]},
+        "sweeps_per_s_ratio": {"learned": pl["ms_per_sweep"] / le["ms_per_sweep"],
+                               "fp32_screen": pl["ms_per_sweep"] / sc["ms_per_sweep"]},
         "ess_note": "tau_int by Sokal's automatic window (c=5); with tau of a few hundred sweeps the ESS of one "
-                    "arm has a relative error of tens of percent",
+                    "arm has a relative error of tens of percent, except that the fp32_screen arm repeats the "
+                    "plain arm's decisions (p2_series_equals_plain), so its ratio is exactly the sweep-rate ratio",
         "seconds_total": time.perf_counter() - t_start}
 
 

@@ -249,6 +249,35 @@ int lcmc_get_volume_samples(lcmc_ctx *ctx, float *x, float *y, int max_n);
 int lcmc_record_history(lcmc_ctx *ctx, int capacity);
 int lcmc_get_history(lcmc_ctx *ctx, int replica, double *rows, int max_rows);
 
+/* The parameters a replica was created with. */
+int lcmc_get_params(lcmc_ctx *ctx, int replica, lcmc_params *out);
+/* Position of a replica's counter-based random streams: sweep s of a replica
+ * draws from counters (seed, particle, s); set it to resume a run. */
+int lcmc_set_sweep_counter(lcmc_ctx *ctx, int replica, int64_t sweep);
+
+/* The reference's configuration files, byte for byte (host only, no device):
+ * fortSphere.1 as esc_fort1 writes it (MCnptColloid.c:3193-3212) and as
+ * read_initial_configuration reads it (2786-2831: the first n_max particles of
+ * a file holding n_read >= n_max); Configuraciones.dat as print_Trayectoria
+ * (3081-3107) and qmga_mcnvtGB.cnf as print_Qmga (3110-3158) write them,
+ * append = the reference's option 1. */
+int lcmc_write_fort1(const char *path, int n, const double *px, const double *py, const double *pz, const double *ox,
+                     const double *oy, const double *oz, const double box[3], double colloid_radius);
+int lcmc_read_fort1(const char *path, int n_max, double *px, double *py, double *pz, double *ox, double *oy,
+                    double *oz, double box[3], double *colloid_radius, int *n_read);
+int lcmc_write_trajectory(const char *path, int append, int n, const double *px, const double *py, const double *pz,
+                          const double *ox, const double *oy, const double *oz, const double box[3]);
+int lcmc_write_qmga(const char *path, int append, int n, const double *px, const double *py, const double *pz,
+                    const double *ox, const double *oy, const double *oz, const double box[3]);
+/* Restart of one replica: fortSphere.1 at `path` plus a binary sidecar
+ * `path`.lcmc with the exact FP64 state, box, running energy and sweep
+ * counter.  Loading uses the sidecar when present (the resumed run makes
+ * exactly the decisions of the uninterrupted one; its seed must match) and
+ * otherwise the text file, with an FP64 energy recompute, as the reference's
+ * initial_configuration_type 1 restart does. */
+int lcmc_save_restart(lcmc_ctx *ctx, int replica, const char *path);
+int lcmc_load_restart(lcmc_ctx *ctx, int replica, const char *path);
+
 /* ---- allocation-free total energy (no counterpart in the reference) ----
  * Some callers cannot let this library allocate device memory: a host program
  * that has already reserved the GPU's memory for its own pool, or a time-step

@@ -33,7 +33,8 @@ SOURCES = {
     "lcmc_noalloc.cu": ["-fmad=false"],
     "lcmc_mlp.cu": [],
     "lcmc_da.cu": [],
-    "lcmc_screen.cu": ["-fmad=false"],  # forms the scaled vectors exactly as the volume scaling does
+    "lcmc_screen.cu": ["-fmad=false"],
+    "lcmc_io.cu": [],  # forms the scaled vectors exactly as the volume scaling does
 }
 
 

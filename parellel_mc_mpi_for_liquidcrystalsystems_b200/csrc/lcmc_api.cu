@@ -990,6 +990,24 @@ extern "C" int lcmc_get_history(lcmc_ctx *ctx, int replica, double *rows, int ma
     return n;
 }
 
+extern "C" int lcmc_get_params(lcmc_ctx *ctx, int replica, lcmc_params *out)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !out) return LCMC_EINVAL;
+    *out = ctx->params[replica];
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_set_sweep_counter(lcmc_ctx *ctx, int replica, int64_t sweep)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || sweep < 0) return LCMC_EINVAL;
+    Replica &rp = ctx->rep[replica];
+    rp.sweep = (unsigned long long)sweep;
+    CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * replica + offsetof(Replica, sweep), &rp.sweep,
+                                  sizeof(rp.sweep), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return LCMC_OK;
+}
+
 extern "C" int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4])
 {
     if (!ctx || !ms) return LCMC_EINVAL;

@@ -196,6 +196,34 @@ class GBSystem:
             self._check(n)
         return rows[:n]
 
+    # -- files (the reference's formats) --
+    def esc_fort1(self, path="fortSphere.1", replica=0):
+        """Write fortSphere.1 as esc_fort1 (MCnptColloid.c:3193-3212) does."""
+        (a, box) = self.download(replica)
+        self._check(lib().lcmc_write_fort1(str(path).encode(), len(a[0]), *[x.ctypes.data_as(_lib.DP) for x in a],
+                                           box.ctypes.data_as(_lib.DP), float(self.params[replica].colloid_radius)))
+
+    def print_Trayectoria(self, path="Configuraciones.dat", append=True, replica=0):
+        """Append (or start) a snapshot as print_Trayectoria (3081-3107) does."""
+        (a, box) = self.download(replica)
+        self._check(lib().lcmc_write_trajectory(str(path).encode(), int(append), len(a[0]),
+                                                *[x.ctypes.data_as(_lib.DP) for x in a], box.ctypes.data_as(_lib.DP)))
+
+    def print_Qmga(self, path="qmga_mcnvtGB.cnf", append=False, replica=0):
+        """Write a QMGA snapshot as print_Qmga (3110-3158) does."""
+        (a, box) = self.download(replica)
+        self._check(lib().lcmc_write_qmga(str(path).encode(), int(append), len(a[0]),
+                                          *[x.ctypes.data_as(_lib.DP) for x in a], box.ctypes.data_as(_lib.DP)))
+
+    def save_restart(self, path="fortSphere.1", replica=0):
+        """fortSphere.1 plus the exact sidecar (path + '.lcmc')."""
+        self._check(lib().lcmc_save_restart(self._h, replica, str(path).encode()))
+
+    def load_restart(self, path="fortSphere.1", replica=0):
+        """Resume from save_restart's files (exactly, with the sidecar), or
+        start from a plain fortSphere.1 (read_initial_configuration)."""
+        self._check(lib().lcmc_load_restart(self._h, replica, str(path).encode()))
+
     # -- measurement --
     def stream_handle(self):
         """cudaStream_t of this context (as an integer) for event timing."""
