@@ -249,6 +249,18 @@ int lcmc_get_volume_samples(lcmc_ctx *ctx, float *x, float *y, int max_n);
 int lcmc_record_history(lcmc_ctx *ctx, int capacity);
 int lcmc_get_history(lcmc_ctx *ctx, int replica, double *rows, int max_rows);
 
+/* Adaptive step (MCnptColloid.c:987-1031), for equilibration only (off by
+ * default, off in parity and production runs): after every block of at least
+ * 10,000 attempts (whole sweeps) a replica's max displacement shrinks by 5 %
+ * below 30 % acceptance and grows by 5 % above 55 %, with the reference's
+ * resets at 1e-4 and 1.5 min(sigma_ee, sigma_ss) (which also scale the
+ * rotation), and never grows beyond its value at creation, which the
+ * checkerboard's cell width was sized for.  Changes the trial moves, so a run
+ * with it on is not a Markov chain with fixed moves: equilibrate with it, then
+ * switch it off. */
+int lcmc_set_adaptive_step(lcmc_ctx *ctx, int on);
+/* Current max displacement and rotation of a replica. */
+int lcmc_get_step(lcmc_ctx *ctx, int replica, double *max_displacement, double *max_rotation);
 /* The parameters a replica was created with. */
 int lcmc_get_params(lcmc_ctx *ctx, int replica, lcmc_params *out);
 /* Position of a replica's counter-based random streams: sweep s of a replica

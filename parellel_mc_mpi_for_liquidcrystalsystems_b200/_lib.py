@@ -96,6 +96,8 @@ EXPORTS = {
     "lcmc_set_surrogate": ([C.c_void_p, C.c_void_p, C.c_double], C.c_int),
     "lcmc_set_fp32_screen": ([C.c_void_p, C.c_int], C.c_int),
     "lcmc_get_params": ([C.c_void_p, C.c_int, C.POINTER(Params)], C.c_int),
+    "lcmc_set_adaptive_step": ([C.c_void_p, C.c_int], C.c_int),
+    "lcmc_get_step": ([C.c_void_p, C.c_int, DP, DP], C.c_int),
     "lcmc_set_sweep_counter": ([C.c_void_p, C.c_int, C.c_int64], C.c_int),
     "lcmc_write_fort1": ([C.c_char_p, C.c_int, DP, DP, DP, DP, DP, DP, DP, C.c_double], C.c_int),
     "lcmc_read_fort1": ([C.c_char_p, C.c_int, DP, DP, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_int)], C.c_int),

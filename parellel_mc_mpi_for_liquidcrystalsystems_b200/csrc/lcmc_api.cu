@@ -575,6 +575,8 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
         rp.pressure = p.system_pressure;
         rp.dlnv_max = rp.ensemble == 2 && p.volume_moves_per_sweep > 0 ? p.npt_max_dlnV : 0.0;
         rp.wmin = min_cell_width(p);
+        rp.d_cap = (double)p.max_displacement;
+        rp.min_thick = (double)(float)std::min(p.gb_sigma_sidetoside * p.gb_kappa, p.gb_sigma_sidetoside);
         seed_key(p.rng_seed, rp.key);
         make_consts(p, rp.k);
         const double L = box_length(p);
@@ -988,6 +990,36 @@ extern "C" int lcmc_get_history(lcmc_ctx *ctx, int replica, double *rows, int ma
     int n = (int)order.size() < max_rows ? (int)order.size() : max_rows;
     for (int k = 0; k < n; k++) memcpy(rows + (size_t)9 * k, &h[(size_t)9 * order[k].second], 9 * sizeof(double));
     return n;
+}
+
+extern "C" int lcmc_set_adaptive_step(lcmc_ctx *ctx, int on)
+{
+    if (!ctx) return LCMC_EINVAL;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int r = 0; r < ctx->R; r++) {
+        Replica rp;
+        char *base = (char *)ctx->d_rep + sizeof(Replica) * r;
+        CUDA_TRY(ctx, cudaMemcpy(&rp, base, sizeof(Replica), cudaMemcpyDeviceToHost));
+        rp.adapt_on = on ? 1 : 0;
+        rp.adapt_att = 0ull;
+        rp.adapt_acc = 0ull;
+        CUDA_TRY(ctx, cudaMemcpy(base + offsetof(Replica, adapt_on), &rp.adapt_on,
+                                 offsetof(Replica, d_cap) - offsetof(Replica, adapt_on), cudaMemcpyHostToDevice));
+        ctx->rep[r].adapt_on = rp.adapt_on;
+    }
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_get_step(lcmc_ctx *ctx, int replica, double *max_displacement, double *max_rotation)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !max_displacement || !max_rotation) return LCMC_EINVAL;
+    GBConsts k;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(&k, (char *)ctx->d_rep + sizeof(Replica) * replica + offsetof(Replica, k),
+                             sizeof(GBConsts), cudaMemcpyDeviceToHost));
+    *max_displacement = k.max_disp;
+    *max_rotation = k.max_rot;
+    return LCMC_OK;
 }
 
 extern "C" int lcmc_get_params(lcmc_ctx *ctx, int replica, lcmc_params *out)

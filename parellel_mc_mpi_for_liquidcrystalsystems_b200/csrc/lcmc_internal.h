@@ -41,6 +41,11 @@ struct Replica {
     // delayed acceptance with the learned surrogate
     int da_on;         // a stage-1 screen is set for this replica
     int da_kind;       // 1 the learned surrogate, 2 the FP32-pair energy change
+    // adaptive step (equilibration only): block counters, the cell grid's cap
+    // on the displacement (creation value) and min(sigma_ee, sigma_ss)
+    int adapt_on;
+    unsigned long long adapt_att, adapt_acc;
+    double d_cap, min_thick;
     int vol_stage1;    // this sweep: 0 rejected by the screen, 1 no screen, 2 passed the screen
     double da_scale;   // surrogate output -> dU / N
     double vol_dU_sur; // surrogate dU of this sweep's move

@@ -311,6 +311,35 @@ __global__ void __launch_bounds__(256) k_sweep_finalize(DevView v)
         st.energy += s[0];
         if (!(s[0] == s[0]) || s[0] - s[0] != 0.0) st.flags |= F_NONFINITE;
         p.sweep += 1ull;
+        // adaptive step (MCnptColloid.c:987-1031) per block of >= 10,000
+        // attempts: -5 % below 30 % acceptance, +5 % above 55 %, with the
+        // reference's resets at 1e-4 and 1.5 min_thick; never above the cap the
+        // cell grid was built for (the checkerboard needs width >= rc + d)
+        if (p.adapt_on) {
+            p.adapt_att += (unsigned long long)p.n;
+            p.adapt_acc += (unsigned long long)s[1];
+            if (p.adapt_att >= 10000ull) {
+                const double ratio = (double)p.adapt_acc / (double)p.adapt_att;
+                p.adapt_att = 0ull;
+                p.adapt_acc = 0ull;
+                double d = p.k.max_disp, a = p.k.max_rot;
+                if (ratio < 0.3) {
+                    d -= d * 0.05;
+                    if (d < 0.0001 * p.min_thick) {
+                        d = 0.01 * p.min_thick;
+                        if (a > 0.000001) a -= 0.5 * a;
+                    }
+                } else if (ratio > 0.55) {
+                    d += d * 0.05;
+                    if (d > 1.5 * p.min_thick) {
+                        d = 0.75 * p.min_thick;
+                        if (a < 0.7) a += 0.5 * a;
+                    }
+                }
+                p.k.max_disp = d < p.d_cap ? d : p.d_cap;
+                p.k.max_rot = a;
+            }
+        }
     }
 }
 

@@ -123,6 +123,17 @@ class GBSystem:
         """n_sweeps checkerboard sweeps (N attempts each) on every replica."""
         self._check(lib().lcmc_sweep(self._h, n_sweeps))
 
+    def set_adaptive_step(self, on=True):
+        """Adaptive max displacement/rotation (MCnptColloid.c:987-1031), for
+        equilibration only."""
+        self._check(lib().lcmc_set_adaptive_step(self._h, int(bool(on))))
+
+    def step(self, replica=0):
+        """Current (max displacement, max rotation)."""
+        d, a = C.c_double(), C.c_double()
+        self._check(lib().lcmc_get_step(self._h, replica, C.byref(d), C.byref(a)))
+        return d.value, a.value
+
     def set_kernel(self, kernel):
         """-1 automatic, 0 the FP64 kernel, 1 the FP32 kernel."""
         self._check(lib().lcmc_set_kernel(self._h, kernel))

@@ -119,3 +119,47 @@ def test_restart_resumes_exactly(tmp_path):
         a, _ = u.download()
         assert u.stats()["sweeps"] == 0
         assert max(np.max(np.abs(x - y)) for x, y in zip(a, saved)) <= 5e-9
+
+
+def test_adaptive_step_follows_the_reference_rule():
+    """The step after every sweep equals a host replay of MCnptColloid.c:987-1031
+    (blocks of >= 10,000 attempts, +-5 %, resets at 1e-4 / 1.5 sigma_ss) with the
+    cap at the creation value; switched off, it stays put."""
+    # 6 cells per axis of width 4.45 (>= rc + d): about 28 rods per cell
+    kw = dict(COMMON, max_displacement=0.4, max_rotation=0.6)
+    n = 6070
+    p = lcmc.default_params(num_particles=n, system_density=0.32, rng_seed=5, precision_mode=1, **kw)
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(30)
+        s.set_adaptive_step(True)
+        d, a = s.step()
+        cap = d
+        assert d == float(np.float32(0.4)) and a == float(np.float32(0.6))
+        att = acc = 0
+        for _ in range(15):
+            before = s.stats()["accepted"]
+            s.sweep(1)
+            att += n
+            acc += s.stats()["accepted"] - before
+            if att >= 10000:
+                ratio = acc / att
+                att = acc = 0
+                if ratio < 0.3:
+                    d -= d * 0.05
+                    if d < 0.0001 * 1.0:
+                        d = 0.01
+                        if a > 0.000001:
+                            a -= 0.5 * a
+                elif ratio > 0.55:
+                    d += d * 0.05
+                    if d > 1.5:
+                        d = 0.75
+                        if a < 0.7:
+                            a += 0.5 * a
+                d = min(d, cap)
+            assert s.step() == (d, a)
+        assert d < cap  # the dense start accepts < 30 %: the step shrank
+        s.set_adaptive_step(False)
+        s.sweep(5)
+        assert s.step() == (d, a)
