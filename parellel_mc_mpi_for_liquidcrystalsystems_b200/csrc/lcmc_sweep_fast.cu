@@ -14,6 +14,12 @@
 //        + U_coll(n_k) - U_coll(o_k)
 //   c(k, m) = [phi(n_k, n_m) - phi(o_k, n_m)] - [phi(n_k, o_m) - phi(o_k, o_m)]
 //
+// The scan adds, for every earlier partner m, either phi(n_k, n_m) - phi(o_k, n_m)
+// (m accepted) or phi(n_k, o_m) - phi(o_k, o_m) (m rejected), never one and then
+// the correction: a near-overlap term of 1e20 or more that would cancel must not
+// pass through the FP64 sum, whose rounding at that size (1e4 and up) would
+// swamp dE_k.
+//
 // which is exactly E_new - E_old of attempt_monte_carlo_move (MCnptColloid.c:
 // 2491-2563) for the sequential in-cell order (ascending id).  Only the short
 // scan over the accept decisions is sequential.
@@ -37,9 +43,9 @@
 //                and new state over both lists together, lane sums in FP64
 //              pair task: 32 unordered in-cell pairs, 4 terms each
 //              (old/new x old/new), differences formed in FP64
-//   5 sums     warp 0, thread per particle: in-cell row sums -> dE before the
-//              corrections (per-particle trial data was prefetched into
-//              shared memory in step 2)
+//   5 sums     warp 0, thread per particle: static + colloid + later in-cell
+//              partners (per-particle trial data was prefetched into shared
+//              memory in step 2)
 //   6 scan     warp 0: Metropolis decisions in id order with the corrections
 //   7 write    accepted trial states to the FP64 master arrays
 #include <cuda_runtime.h>
@@ -70,7 +76,9 @@ struct FastSmem {
     static constexpr int NPAIR = AMAX * (AMAX - 1) / 2;
     float4 cpos[NW * SEG];     // x, y, z, ux of the static candidates (segment per warp)
     float2 cori[NW * SEG];     // uy, uz
-    float pCA[NPAIR], pBA[NPAIR], pcm[NPAIR]; // in-cell: C-A, B-A, (D-C)-(B-A)
+    // in-cell pair terms rounded to FP32: C - A, B - A, D - C (for a later particle the scan adds
+    // D - C if the earlier partner moved, B - A if it stayed)
+    float pCA[NPAIR], pBA[NPAIR], pDC[NPAIR];
     // old (a) and trial (b) state of each active particle, relative to the cell
     // origin: [0] = (ax, ay, az, aux), [1] = (auy, auz, bx, by), [2] = (bz, bux, buy, buz)
     float4 pst[AMAX][3];
@@ -432,7 +440,7 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
                     const double a = A, b = B, c = Cc, d = D;
                     sm.pCA[idx] = (float)(c - a);
                     sm.pBA[idx] = (float)(b - a);
-                    sm.pcm[idx] = (float)((d - c) - (b - a));
+                    sm.pDC[idx] = (float)(d - c);
                 }
 #pragma unroll
                 for (int o = 16; o >= 1; o >>= 1) npin += __shfl_xor_sync(0xffffffffu, npin, o);
@@ -451,27 +459,20 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
         // ---- 5+6 warp 0: in-cell row sums (thread per particle) -> dE before the
         //      corrections, then the sequential Metropolis scan in id order ----
         if (w == 0) {
+            // decision-independent part of dE_k: static cells, colloid, and the
+            // in-cell partners after k (still at their old state when k is tried)
             double e0 = 0.0, e1 = 0.0;
             for (int h = 0; h < 2; h++) {
                 const int k = lane + 32 * h;
                 if (k >= na) break;
-                // two partial sums per loop: independent FP64 add chains
-                double sa = 0.0, sb = 0.0, sc = 0.0, sd = 0.0;
-                const int kb = tri(0, k);
-                int m = 0;
-                for (; m + 1 < k; m += 2) { // phi(n_k, o_m) - phi(o_k, o_m), k later in the pair
-                    sa += (double)sm.pBA[kb + m];
-                    sb += (double)sm.pBA[kb + m + 1];
-                }
-                if (m < k) sa += (double)sm.pBA[kb + m];
-                m = k + 1;
-                for (; m + 1 < na; m += 2) { // k earlier in the pair
+                double sc = 0.0, sd = 0.0;
+                int m = k + 1;
+                for (; m + 1 < na; m += 2) {
                     sc += (double)sm.pCA[tri(k, m)];
                     sd += (double)sm.pCA[tri(k, m + 1)];
                 }
                 if (m < na) sc += (double)sm.pCA[tri(k, m)];
-                const double s = (sa + sb) + (sc + sd);
-                const double d = (sm.Snew[k] - sm.Sold[k]) + s + sm.tdU[k];
+                const double d = (sm.Snew[k] - sm.Sold[k]) + (sc + sd) + sm.tdU[k];
                 if (h == 0) e0 = d;
                 else e1 = d;
             }
@@ -480,9 +481,19 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             int nacc = 0, nhard = 0;
             for (int m = 0; m < na; m++) {
                 const int own = m & 31;
-                // this step's corrections and draws do not depend on the decision chain
-                const double c0 = (lane > m && lane < na) ? (double)sm.pcm[tri(m, lane)] : 0.0;
-                const double c1 = (lane + 32 > m && lane + 32 < na) ? (double)sm.pcm[tri(m, lane + 32)] : 0.0;
+                // the term partner m adds to each later particle k: D - C if m moves,
+                // B - A if it stays (both loaded before the decision is known)
+                float dc0 = 0.0f, ba0 = 0.0f, dc1 = 0.0f, ba1 = 0.0f;
+                if (lane > m && lane < na) {
+                    const int t0 = tri(m, lane);
+                    dc0 = sm.pDC[t0];
+                    ba0 = sm.pBA[t0];
+                }
+                if (lane + 32 > m && lane + 32 < na) {
+                    const int t1 = tri(m, lane + 32);
+                    dc1 = sm.pDC[t1];
+                    ba1 = sm.pBA[t1];
+                }
                 const double lum = sm.tlu[m];
                 const int hd = sm.hard[m];
                 const double val = __shfl_sync(0xffffffffu, m < 32 ? e0 : e1, own);
@@ -491,9 +502,9 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
                 if (acc) {
                     dsum += val;
                     nacc++;
-                    e0 += c0;
-                    e1 += c1;
                 }
+                e0 += (double)(acc ? dc0 : ba0);
+                e1 += (double)(acc ? dc1 : ba1);
                 if (lane == 0) sm.acc[m] = acc;
             }
             if (lane == 0) {
