@@ -3,8 +3,8 @@
 tests/golden/ensemble_golden.npz holds <U/N> and <P2> (block-averaged, with
 standard errors) of a long run of the reference's attempt_monte_carlo_move
 (MCnptColloid.c:2445-2604, random particle per attempt) on N = 1728 rods at
-rho* = 0.10, T* = 1.0 with a colloid of radius 2 (made by
-tests/golden/make_ensemble_golden.py).  The checkerboard sweeps here sample
+rho* = 0.10, T* = 2.0, step 0.5 and rotation 0.3, with a colloid of radius 2
+(made by tests/golden/make_ensemble_golden.py).  The checkerboard sweeps here sample
 the same Boltzmann distribution with a different move schedule; 16 replicas
 from the same lattice start, each with its own seed, give means whose
 standard error comes from the spread of the replica means.  Both must agree
@@ -28,20 +28,27 @@ def test_ensemble_matches_reference_chain(golden, precision):
     n = int(g["n"])
     common = dict(num_particles=n, system_density=float(g["rho"]), system_temperature=float(g["T"]),
                   colloid_wall_option=1, colloid_radius=float(g["colloid_R"]), gb_kappa=3.0, gb_kappa_prime=5.0,
-                  gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0, max_displacement=0.1,
-                  max_rotation=0.1, precision_mode=precision)
+                  gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
+                  max_displacement=float(g["dmax"]), max_rotation=float(g["rot"]), precision_mode=precision)
     start, box = lcmc.lattice(lcmc.default_params(rng_seed=int(g["seed"]), **common))
     ps = [lcmc.default_params(rng_seed=9000 + 17 * r, **common) for r in range(REPLICAS)]
     with lcmc.GBSystem(ps) as s:
         for r in range(REPLICAS):
             s.upload(*start, box, replica=r)
         s.sweep(BURN)
+        # the lattice start relaxes from overlap energies of ~1e10: restart the
+        # running energies from an FP64 recompute before the production sweeps
+        for r in range(REPLICAS):
+            s.tot_ene(r)
         s.record_history(SWEEPS)
         s.sweep(SWEEPS)
         u = np.array([da.p2_series(s, r)[2].mean() / n for r in range(REPLICAS)])
         p2 = np.array([da.p2_series(s, r)[1].mean() for r in range(REPLICAS)])
         drift = max(abs(s.stats(r)["energy"] - s.tot_ene(r)) / n for r in range(REPLICAS))
-    assert drift < (1e-5 if precision == 1 else 1e-9)  # running energy vs FP64 recompute, per particle
+    # running energy after the production sweeps vs an FP64 recompute, per
+    # particle: FP32 pair terms leave ~4e-5 kT of rounding in each dE, which
+    # adds up as a random walk over the ~3e6 accepted moves of a replica
+    assert drift < (1e-4 if precision == 1 else 1e-9), drift
     for name, gpu, ref_m, ref_se in (("U/N", u, float(g["u_mean"]), float(g["u_se"])),
                                      ("P2", p2, float(g["p2_mean"]), float(g["p2_se"]))):
         m, se = gpu.mean(), gpu.std(ddof=1) / np.sqrt(len(gpu))
