@@ -46,7 +46,8 @@
 //   5 sums     warp 0, thread per particle: static + colloid + later in-cell
 //              partners (per-particle trial data was prefetched into shared
 //              memory in step 2)
-//   6 scan     warp 0: Metropolis decisions in id order with the corrections
+//   6 decide   warp 0: Metropolis decisions in id order (fixed-point rounds of
+//              the triangular system the sequential order defines)
 //   7 write    accepted trial states to the FP64 master arrays
 #include <cuda_runtime.h>
 
@@ -456,8 +457,8 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             continue;
         }
 
-        // ---- 5+6 warp 0: in-cell row sums (thread per particle) -> dE before the
-        //      corrections, then the sequential Metropolis scan in id order ----
+        // ---- 5+6 warp 0: decision-independent part of dE (thread per particle),
+        //      then the Metropolis decisions in id order ----
         if (w == 0) {
             // decision-independent part of dE_k: static cells, colloid, and the
             // in-cell partners after k (still at their old state when k is tried)
@@ -476,37 +477,48 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
                 if (h == 0) e0 = d;
                 else e1 = d;
             }
+            // Metropolis decisions in id order.  dE_k = base_k + sum over earlier
+            // m of (D - C if m accepted, else B - A): a triangular system, solved
+            // by fixed-point rounds in parallel.  Each round recomputes every
+            // dE_k from the current guess of the earlier decisions, adding the
+            // terms in increasing m exactly as a sequential scan would; after
+            // round r the first r decisions are final, and a round that changes
+            // no decision has reached the unique solution (usually round 2 or
+            // 3), so the decisions and dE_k equal the sequential scan's bits.
             const double beta = p.k.beta;
-            double dsum = 0.0;
-            int nacc = 0, nhard = 0;
-            for (int m = 0; m < na; m++) {
-                const int own = m & 31;
-                // the term partner m adds to each later particle k: D - C if m moves,
-                // B - A if it stays (both loaded before the decision is known)
-                float dc0 = 0.0f, ba0 = 0.0f, dc1 = 0.0f, ba1 = 0.0f;
-                if (lane > m && lane < na) {
-                    const int t0 = tri(m, lane);
-                    dc0 = sm.pDC[t0];
-                    ba0 = sm.pBA[t0];
+            const bool v0 = lane < na, v1 = lane + 32 < na;
+            const unsigned hd0 = __ballot_sync(0xffffffffu, v0 && sm.hard[lane]);
+            const unsigned hd1 = __ballot_sync(0xffffffffu, v1 && sm.hard[lane + 32]);
+            const double lu0 = v0 ? sm.tlu[lane] : 0.0, lu1 = v1 ? sm.tlu[lane + 32] : 0.0;
+            unsigned acc0 = 0u, acc1 = 0u;
+            double x0 = e0, x1 = e1;
+            for (int round = 0; round <= na; round++) {
+                x0 = e0;
+                x1 = e1;
+                if (v0) {
+                    const int kb = tri(0, lane);
+                    for (int m = 0; m < lane; m++) x0 += (double)((acc0 >> m) & 1u ? sm.pDC[kb + m] : sm.pBA[kb + m]);
                 }
-                if (lane + 32 > m && lane + 32 < na) {
-                    const int t1 = tri(m, lane + 32);
-                    dc1 = sm.pDC[t1];
-                    ba1 = sm.pBA[t1];
+                if (v1) {
+                    const int k = lane + 32, kb = tri(0, k);
+                    for (int m = 0; m < 32; m++) x1 += (double)((acc0 >> m) & 1u ? sm.pDC[kb + m] : sm.pBA[kb + m]);
+                    for (int m = 32; m < k; m++)
+                        x1 += (double)((acc1 >> (m - 32)) & 1u ? sm.pDC[kb + m] : sm.pBA[kb + m]);
                 }
-                const double lum = sm.tlu[m];
-                const int hd = sm.hard[m];
-                const double val = __shfl_sync(0xffffffffu, m < 32 ? e0 : e1, own);
-                const bool acc = !hd && ((val <= 0.0) || (lum <= -beta * val));
-                nhard += hd;
-                if (acc) {
-                    dsum += val;
-                    nacc++;
-                }
-                e0 += (double)(acc ? dc0 : ba0);
-                e1 += (double)(acc ? dc1 : ba1);
-                if (lane == 0) sm.acc[m] = acc;
+                const bool a0 = v0 && !((hd0 >> lane) & 1u) && ((x0 <= 0.0) || (lu0 <= -beta * x0));
+                const bool a1 = v1 && !((hd1 >> lane) & 1u) && ((x1 <= 0.0) || (lu1 <= -beta * x1));
+                const unsigned n0 = __ballot_sync(0xffffffffu, a0), n1 = __ballot_sync(0xffffffffu, a1);
+                if (n0 == acc0 && n1 == acc1) break;
+                acc0 = n0;
+                acc1 = n1;
             }
+            if (v0) sm.acc[lane] = (acc0 >> lane) & 1u;
+            if (v1) sm.acc[lane + 32] = (acc1 >> lane) & 1u;
+            // accepted dE summed in a fixed (butterfly) order
+            double dsum = ((acc0 >> lane) & 1u ? x0 : 0.0) + ((acc1 >> lane) & 1u ? x1 : 0.0);
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+            const int nacc = __popc(acc0) + __popc(acc1), nhard = __popc(hd0) + __popc(hd1);
             if (lane == 0) {
                 if (!(dsum - dsum == 0.0)) atomicOr(&v.stats[r].flags, F_NONFINITE);
                 v.cell_e0[cell] = dsum;
