@@ -535,7 +535,7 @@ static void choose_kernels(lcmc_ctx *c)
         if (rp.ensemble == 2) c->any_npt = true;
         spec21 = spec21 && p.gb_mu_exponent == 2.0 && p.gb_nu_exponent == 1.0 && p.gb_sigma_sidetoside == 1.0;
     }
-    c->fast_variant = 2 * (need_amax > 48 ? 1 : 0) + (spec21 ? 1 : 0);
+    c->fast_variant = 2 * (need_amax > fast_variant(0).amax ? 1 : 0) + (spec21 ? 1 : 0);
 }
 
 static int upload_replica_table(lcmc_ctx *c)

@@ -17,7 +17,7 @@ int energy_exact_blocks_per_sm(); // resident blocks of 128 threads per SM
 
 // lcmc_sweep_fast.cu (FP32)
 struct FastVariant {
-    int threads, cpl, amax, lcap;
+    int threads, amax, seg, lcap; // active-cell capacity, staged candidates per warp, list capacity
 };
 int fast_variant_count();
 FastVariant fast_variant(int i);

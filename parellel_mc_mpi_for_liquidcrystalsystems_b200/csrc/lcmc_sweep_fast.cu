@@ -85,7 +85,6 @@ struct FastSmem {
     float4 pst[AMAX][3];
     float rad2[AMAX];
     double Sold[AMAX], Snew[AMAX];
-    double tn[6][AMAX];   // trial state (FP64 master values written on acceptance)
     double tdU[AMAX], tlu[AMAX]; // colloid dU of the trial, log of the Metropolis draw
     int pid[AMAX];        // particle id (outcome slot)
     unsigned char hard[AMAX];
@@ -109,12 +108,18 @@ __device__ __forceinline__ void cell_failed(const DevView &v, int r, int cell, i
     v.cell_cands[cell] = 0ull;
 }
 
+// resident CTAs per SM the register budget is sized for: the small capacity
+// class (36.9 KB of shared memory) fits six per SM at 80 registers, the large
+// class is limited to three by its shared memory
+template <int AMAX> struct FastMinBlocks { static constexpr int value = AMAX <= 48 ? 6 : 3; };
+
 template <int NT, int AMAX, int SEG, int LW, bool SPEC21>
-__global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
+__global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(DevView v, int ci)
 {
     using SM = FastSmem<NT, AMAX, SEG, LW>;
     constexpr int NW = SM::NW;
     static_assert(AMAX <= 64, "the scan warp holds two particles per lane");
+    static_assert(AMAX + 32 <= NT, "threads 32 .. 32 + AMAX - 1 write the particles back");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SM &sm = *reinterpret_cast<SM *>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -193,12 +198,6 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
             const unsigned char hd = v.thard[g];
             sm.rad2[k] = hd ? -1.0f : rr * rr;
             sm.hard[k] = hd;
-            sm.tn[0][k] = v.tnx[g];
-            sm.tn[1][k] = v.tny[g];
-            sm.tn[2][k] = v.tnz[g];
-            sm.tn[3][k] = v.tux[g];
-            sm.tn[4][k] = v.tuy[g];
-            sm.tn[5][k] = v.tuz[g];
             sm.tdU[k] = v.tdU[g];
             sm.tlu[k] = v.tlu[g];
             sm.pid[k] = v.id[g];
@@ -458,7 +457,19 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
         }
 
         // ---- 5+6 warp 0: decision-independent part of dE (thread per particle),
-        //      then the Metropolis decisions in id order ----
+        //      then the Metropolis decisions in id order; meanwhile thread
+        //      32 + k loads the FP64 trial state of particle k for step 7 ----
+        const int kw = t - 32; // write-back particle of this thread
+        double wn[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (w != 0 && kw < na) {
+            const int g = g0 + kw;
+            wn[0] = v.tnx[g];
+            wn[1] = v.tny[g];
+            wn[2] = v.tnz[g];
+            wn[3] = v.tux[g];
+            wn[4] = v.tuy[g];
+            wn[5] = v.tuz[g];
+        }
         if (w == 0) {
             // decision-independent part of dE_k: static cells, colloid, and the
             // in-cell partners after k (still at their old state when k is tried)
@@ -531,16 +542,16 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
         __syncthreads();
 
         // ---- 7 write-back ----
-        for (int k = t; k < na; k += NT) {
-            const int g = g0 + k;
+        if (w != 0 && kw < na) {
+            const int k = kw, g = g0 + k;
             const int acc = sm.acc[k];
             if (acc) {
-                v.px[g] = sm.tn[0][k];
-                v.py[g] = sm.tn[1][k];
-                v.pz[g] = sm.tn[2][k];
-                v.ox[g] = sm.tn[3][k];
-                v.oy[g] = sm.tn[4][k];
-                v.oz[g] = sm.tn[5][k];
+                v.px[g] = wn[0];
+                v.py[g] = wn[1];
+                v.pz[g] = wn[2];
+                v.ox[g] = wn[3];
+                v.oy[g] = wn[4];
+                v.oz[g] = wn[5];
                 const float4 P1 = sm.pst[k][1], P2 = sm.pst[k][2];
                 v.cl4[g] = make_float4(P1.z, P1.w, P2.x, P2.y);
                 v.cl2[g] = make_float2(P2.z, P2.w);
@@ -558,7 +569,7 @@ __global__ void __launch_bounds__(NT, 5) k_phase_fast(DevView v, int ci)
 namespace lcmc {
 
 // (threads, active capacity, staged candidates per warp segment, per-warp list capacity)
-static const FastVariant kVariants[] = {{128, 48, 192, 256}, {128, 64, 288, 384}};
+static const FastVariant kVariants[] = {{128, 48, 176, 160}, {128, 64, 288, 384}};
 
 int fast_variant_count() { return (int)(sizeof(kVariants) / sizeof(kVariants[0])); }
 FastVariant fast_variant(int i) { return kVariants[i]; }
@@ -575,6 +586,8 @@ static int occupancy_v()
 {
     const int bytes = (int)sizeof(FastSmem<NT, AMAX, SEG, LW>);
     cudaFuncSetAttribute(k_phase_fast<NT, AMAX, SEG, LW, S21>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_phase_fast<NT, AMAX, SEG, LW, S21>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_phase_fast<NT, AMAX, SEG, LW, S21>, NT, bytes);
     return n > 0 ? n : 1;
@@ -584,8 +597,8 @@ static int occupancy_v()
 void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, int grid)
 {
     switch (variant) {
-    case 0: launch_v<128, 48, 192, 256, false>(v, s, ci, grid); break;
-    case 1: launch_v<128, 48, 192, 256, true>(v, s, ci, grid); break;
+    case 0: launch_v<128, 48, 176, 160, false>(v, s, ci, grid); break;
+    case 1: launch_v<128, 48, 176, 160, true>(v, s, ci, grid); break;
     case 2: launch_v<128, 64, 288, 384, false>(v, s, ci, grid); break;
     default: launch_v<128, 64, 288, 384, true>(v, s, ci, grid); break;
     }
@@ -596,8 +609,8 @@ void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, in
 int fast_blocks_per_sm(int variant)
 {
     switch (variant) {
-    case 0: return occupancy_v<128, 48, 192, 256, false>();
-    case 1: return occupancy_v<128, 48, 192, 256, true>();
+    case 0: return occupancy_v<128, 48, 176, 160, false>();
+    case 1: return occupancy_v<128, 48, 176, 160, true>();
     case 2: return occupancy_v<128, 64, 288, 384, false>();
     default: return occupancy_v<128, 64, 288, 384, true>();
     }
