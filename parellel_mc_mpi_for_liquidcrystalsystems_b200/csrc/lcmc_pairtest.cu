@@ -11,27 +11,17 @@ __global__ void k_pair_terms32(GBConsts k, int n, const double *d, const double 
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    FastK K;
-    K.rc2 = k.f_rc2;
-    K.chi = k.f_chi;
-    K.chi_sq = k.f_chi_sq;
-    K.chip = k.f_chip;
-    K.chip_sq = k.f_chip_sq;
-    K.sigma0 = k.f_sigma0;
-    K.four_eps0 = k.f_4eps0;
-    K.half_chi = k.f_half_chi;
-    K.half_chip = k.f_half_chip;
-    K.mu_code = k.mu_code;
-    K.nu_code = k.nu_code;
-    K.mu = (float)k.mu;
-    K.nu = (float)k.nu;
+    const FastK K = fast_consts(k);
+    const bool spec21 = k.mu_code == 2 && k.nu_code == 1 && k.f_sigma0 == 1.0f;
     float dx = (float)d[3 * i], dy = (float)d[3 * i + 1], dz = (float)d[3 * i + 2];
     float r2 = dx * dx + dy * dy + dz * dz;
     double ni = sqrt(ei[3 * i] * ei[3 * i] + ei[3 * i + 1] * ei[3 * i + 1] + ei[3 * i + 2] * ei[3 * i + 2]);
     double nj = sqrt(ej[3 * i] * ej[3 * i] + ej[3 * i + 1] * ej[3 * i + 1] + ej[3 * i + 2] * ej[3 * i + 2]);
-    float e = pair_fast(K, dx, dy, dz, r2, (float)(ei[3 * i] / ni), (float)(ei[3 * i + 1] / ni),
-                        (float)(ei[3 * i + 2] / ni), (float)(ej[3 * i] / nj), (float)(ej[3 * i + 1] / nj),
-                        (float)(ej[3 * i + 2] / nj));
+    const float a0 = (float)(ei[3 * i] / ni), a1 = (float)(ei[3 * i + 1] / ni), a2 = (float)(ei[3 * i + 2] / ni);
+    const float b0 = (float)(ej[3 * i] / nj), b1 = (float)(ej[3 * i + 1] / nj), b2 = (float)(ej[3 * i + 2] / nj);
+    // the specialised term the sweep kernels run for GB(kappa, kappa', 2, 1), else the general one
+    float e = spec21 ? pair_fast_t<true>(K, dx, dy, dz, r2, a0, a1, a2, b0, b1, b2)
+                     : pair_fast_t<false>(K, dx, dy, dz, r2, a0, a1, a2, b0, b1, b2);
     out[i] = r2 < K.rc2 ? (double)e : 0.0;
 }
 

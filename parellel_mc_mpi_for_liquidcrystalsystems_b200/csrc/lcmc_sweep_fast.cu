@@ -39,8 +39,9 @@
 //              particle task (two particles k, k + 1): cutoff test of every
 //                staged candidate, loaded once, against both old positions
 //                with radius rc + |displacement| (covers old and new state),
-//                ballot compaction into two lists, then FP32 Gay-Berne for old
-//                and new state over both lists together, lane sums in FP64
+//                warp segment by warp segment, ballot compaction into two
+//                lists, then FP32 Gay-Berne for old and new state over both
+//                lists together, lane sums in FP64
 //              pair task: 32 unordered in-cell pairs, 4 terms each
 //              (old/new x old/new), differences formed in FP64
 //   5 sums     warp 0, thread per particle: static + colloid + later in-cell
@@ -269,25 +270,8 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
             __syncthreads();
             continue;
         }
-        int segc[NW];
-#pragma unroll
-        for (int i = 0; i < NW; i++) segc[i] = sm.segcnt[i];
-
         // ---- 4 task queue: particle tasks (two particles each: cutoff test +
         //      pair sums) and in-cell pair tasks ----
-        // staged candidates as one flat index f over the warp segments:
-        // slot = f - segoff[i] for the segment i holding f
-        int segp[NW], segoff[NW];
-        {
-            int acc_ = 0;
-#pragma unroll
-            for (int i = 0; i < NW; i++) {
-                segp[i] = acc_;
-                segoff[i] = acc_ - i * SEG;
-                acc_ += segc[i];
-            }
-        }
-        const int stot = segp[NW - 1] + segc[NW - 1];
         const int nptask = (na + 1) >> 1;
         const int npair = na * (na - 1) / 2;
         const int ntask = nptask + (npair + 31) / 32;
@@ -302,44 +286,43 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                 const bool has_b = kb < na;
                 const float R2a = sm.rad2[ka];
                 const float R2b = has_b ? sm.rad2[kb] : -1.0f;
-                const float4 qa = sm.pst[ka][0];
-                const float4 qb = has_b ? sm.pst[kb][0] : qa;
                 double soa = 0.0, sna = 0.0, sob = 0.0, snb = 0.0;
                 int np = 0;
                 if (R2a > 0.0f || R2b > 0.0f) {
+                    const float4 qa = sm.pst[ka][0];
+                    const float4 qb = has_b ? sm.pst[kb][0] : qa;
                     int ca = 0, cb = 0;
-                    for (int base = 0; base < stot; base += 64) {
-                        bool pa[2], pb[2];
-                        int sl[2];
+                    // cutoff test of every staged candidate, warp segment by warp segment
+#pragma unroll 1
+                    for (int i = 0; i < NW; i++) {
+                        const int s0 = i * SEG, sc = sm.segcnt[i];
+                        for (int base = 0; base < sc; base += 64) {
+                            bool pa[2], pb[2];
 #pragma unroll
-                        for (int h = 0; h < 2; h++) {
-                            const int f = base + 32 * h + lane;
-                            pa[h] = pb[h] = false;
-                            sl[h] = 0;
-                            if (f < stot) {
-                                int o = segoff[0];
-#pragma unroll
-                                for (int i = 1; i < NW; i++)
-                                    if (f >= segp[i]) o = segoff[i];
-                                sl[h] = f - o;
-                                const float4 c = sm.cpos[sl[h]];
-                                float dx = c.x - qa.x, dy = c.y - qa.y, dz = c.z - qa.z;
-                                pa[h] = dx * dx + dy * dy + dz * dz < R2a;
-                                dx = c.x - qb.x;
-                                dy = c.y - qb.y;
-                                dz = c.z - qb.z;
-                                pb[h] = dx * dx + dy * dy + dz * dz < R2b;
+                            for (int h = 0; h < 2; h++) {
+                                const int j = base + 32 * h + lane;
+                                pa[h] = pb[h] = false;
+                                if (j < sc) {
+                                    const float4 c = sm.cpos[s0 + j];
+                                    float dx = c.x - qa.x, dy = c.y - qa.y, dz = c.z - qa.z;
+                                    pa[h] = dx * dx + dy * dy + dz * dz < R2a;
+                                    dx = c.x - qb.x;
+                                    dy = c.y - qb.y;
+                                    dz = c.z - qb.z;
+                                    pb[h] = dx * dx + dy * dy + dz * dz < R2b;
+                                }
                             }
-                        }
 #pragma unroll
-                        for (int h = 0; h < 2; h++) {
-                            const unsigned ba = __ballot_sync(0xffffffffu, pa[h]);
-                            const unsigned bb = __ballot_sync(0xffffffffu, pb[h]);
-                            const int pa_ = ca + __popc(ba & lt), pb_ = cb + __popc(bb & lt);
-                            if (pa[h] && pa_ < LW) sm.wlist[w][0][pa_] = (unsigned short)sl[h];
-                            if (pb[h] && pb_ < LW) sm.wlist[w][1][pb_] = (unsigned short)sl[h];
-                            ca += __popc(ba);
-                            cb += __popc(bb);
+                            for (int h = 0; h < 2; h++) {
+                                const unsigned ba = __ballot_sync(0xffffffffu, pa[h]);
+                                const unsigned bb = __ballot_sync(0xffffffffu, pb[h]);
+                                const int pa_ = ca + __popc(ba & lt), pb_ = cb + __popc(bb & lt);
+                                const unsigned short sl = (unsigned short)(s0 + base + 32 * h + lane);
+                                if (pa[h] && pa_ < LW) sm.wlist[w][0][pa_] = sl;
+                                if (pb[h] && pb_ < LW) sm.wlist[w][1][pb_] = sl;
+                                ca += __popc(ba);
+                                cb += __popc(bb);
+                            }
                         }
                     }
                     if (ca > LW || cb > LW) {
