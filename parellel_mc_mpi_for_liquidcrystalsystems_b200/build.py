@@ -33,8 +33,10 @@ SOURCES = {
     "lcmc_noalloc.cu": ["-fmad=false"],
     "lcmc_mlp.cu": [],
     "lcmc_da.cu": [],
-    "lcmc_screen.cu": ["-fmad=false"],
-    "lcmc_io.cu": [],  # forms the scaled vectors exactly as the volume scaling does
+    # FP32 pair terms contract freely; its FP64 distance and scaling use rounded
+    # intrinsics (the FP64 kernel's arithmetic in any contraction setting)
+    "lcmc_screen.cu": [],
+    "lcmc_io.cu": [],
 }
 
 

@@ -27,16 +27,19 @@ __device__ __forceinline__ double g_omega_d(double eiej, double amasb2, double a
 __device__ __forceinline__ double dist_fold(double xi, double yi, double zi, double xj, double yj, double zj,
                                             const double L[3], double d[3])
 {
-    d[0] = xj - xi;
-    d[1] = yj - yi;
-    d[2] = zj - zi;
+    // rounded operations throughout, so the result is the same in every
+    // translation unit whatever its contraction setting
+    d[0] = __dsub_rn(xj, xi);
+    d[1] = __dsub_rn(yj, yi);
+    d[2] = __dsub_rn(zj, zi);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        if (d[a] > 0.5 * L[a]) d[a] -= L[a];
-        else if (d[a] < -0.5 * L[a]) d[a] += L[a];
+        const double h = __dmul_rn(0.5, L[a]);
+        if (d[a] > h) d[a] = __dsub_rn(d[a], L[a]);
+        else if (d[a] < -h) d[a] = __dadd_rn(d[a], L[a]);
     }
-    double xs = d[0] * d[0], ys = d[1] * d[1], zs = d[2] * d[2];
-    return xs + ys + zs;
+    const double xs = __dmul_rn(d[0], d[0]), ys = __dmul_rn(d[1], d[1]), zs = __dmul_rn(d[2], d[2]);
+    return __dadd_rn(__dadd_rn(xs, ys), zs);
 }
 
 // Pair term for r^2 < rc^2 (the caller tests the cutoff), orientations of any norm.
