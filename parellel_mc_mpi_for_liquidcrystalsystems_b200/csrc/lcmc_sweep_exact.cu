@@ -17,6 +17,7 @@
 #include "lcmc_internal.h"
 #include "lcmc_rng.cuh"
 #include "lcmc_trial.cuh"
+#include "lcmc_volume_cells.cuh"
 
 namespace lcmc {
 
@@ -199,11 +200,20 @@ __global__ void __launch_bounds__(128, LCMC_ENERGY_MIN_BLOCKS) k_energy_exact(De
     __shared__ int s_start[4][28]; // flat index of the first candidate of each cell
     __shared__ int s_base[4][28];  // particle slot minus flat index, per cell
     __shared__ int s_qj[4][EQ];    // queued candidate slot, configuration in bit 31
+    if (SCALED) { // nothing to do when the cell kernel serves every NPT replica needing the energies
+        bool any = false;
+        for (int r = 0; r < v.R && !any; r++) {
+            const Replica &p = v.rep[r];
+            any = p.ensemble == 2 && !(p.da_on && !p.vol_stage1) && !volume_cells_serves<true>(p);
+        }
+        if (!any) return;
+    }
     for (int i = blockIdx.x * nw + wib; i < v.ntot; i += gridDim.x * nw) {
         const int r = v.p2r[i];
         const Replica &p = v.rep[r];
         const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
-        if (SCALED && (p.ensemble != 2 || (p.da_on && !p.vol_stage1))) continue; // NVT, or screened out
+        // NVT, screened out, or served by the cell kernel (>= 4 cells per axis)
+        if (SCALED && (p.ensemble != 2 || (p.da_on && !p.vol_stage1) || volume_cells_serves<true>(p))) continue;
         const int own = v.scid[i];
         const int cell = own - p.cell_off;
         const int cx = cell % nc0, cy = (cell / nc0) % nc1, cz = cell / (nc0 * nc1);
@@ -342,10 +352,34 @@ int energy_exact_blocks_per_sm()
     return b;
 }
 
+// resident blocks of the cell kernel on this device (queried once)
+static int volume_cells_grid()
+{
+    static int grid = 0;
+    if (!grid) {
+        int dev = 0, sms = 0, b = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_volume_cells<true, false>, 128, 0) != cudaSuccess ||
+            b < 1) {
+            cudaGetLastError();
+            b = 2;
+        }
+        grid = b * (sms > 0 ? sms : 1);
+    }
+    return grid;
+}
+
+// scaled = 1: the volume move's U(V), U(V') -- the cell kernel for systems with
+// >= 4 cells per axis, the per-particle kernel for the rest
 void launch_energy_exact(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int scaled, int grid)
 {
-    if (scaled) k_energy_exact<true><<<grid, 128, 0, s>>>(v, e0, e1, hard);
-    else k_energy_exact<false><<<grid, 128, 0, s>>>(v, e0, e1, hard);
+    if (scaled) {
+        k_volume_cells<true, false><<<volume_cells_grid(), 128, 0, s>>>(v, e0, e1, hard);
+        k_energy_exact<true><<<grid, 128, 0, s>>>(v, e0, e1, hard);
+    } else {
+        k_energy_exact<false><<<grid, 128, 0, s>>>(v, e0, e1, hard);
+    }
 }
 
 } // namespace lcmc

@@ -133,23 +133,28 @@ def test_total_energy_vs_oracle(golden, n, R):
         assert abs(e - float(g["plain_E"])) <= 1e-12 * abs(float(g["plain_E"]))
 
 
-def test_npt_volume_moves_vs_oracle():
-    lp, op = params_pair(1000, 0.30, 31, precision_mode=0, mc_ensemble_type=2, system_pressure=2.0,
+@pytest.mark.parametrize("n,sweeps", [(1000, 4), (11000, 2)])
+def test_npt_volume_moves_vs_oracle(n, sweeps):
+    """N = 1000: 3 cells per axis (per-particle volume-energy kernel); N = 11000:
+    8 cells per axis (cell kernel for the volume move's energies)."""
+    lp, op = params_pair(n, 0.30, 31, precision_mode=0, mc_ensemble_type=2, system_pressure=2.0,
                          system_temperature=0.9, npt_max_dlnV=0.01)
     g_state, box = start_state(lp)
     with lcmc.GBSystem(lp) as s:
         s.set_kernel(0)
         s.upload(*g_state, box)
-        got = gpu_sweeps(s, 4)
+        got = gpu_sweeps(s, sweeps)
         st = s.stats()
         (gx, gy, gz, gox, goy, goz), gbox = s.download()
     state = [x.copy() for x in g_state]
     obox = box.copy()
-    want, vols = oracle_sweeps(op, state, obox, 4, npt=True)
+    want, vols = oracle_sweeps(op, state, obox, sweeps, npt=True)
     for a, b in zip(got, want):
         assert np.array_equal(a, b)
-    assert st["volume_attempted"] == 4
+    assert st["volume_attempted"] == sweeps
     assert st["volume_accepted"] == sum(1 for v in vols if v[0] == 1)
+    # the last sweep's U(V) (volume kernel) against the oracle's, same configuration
+    assert abs(st["last_recompute"] - vols[-1][2]) <= 1e-12 * abs(vols[-1][2])
     assert np.array_equal(bits(gbox), bits(obox))
     for a, b in zip((gx, gy, gz, gox, goy, goz), state):
         assert np.array_equal(bits(a), bits(b))
