@@ -252,7 +252,7 @@ def dilute_start(n, rho0, R, seed):
 def npt_params(lcmc, n, T, P, R, seed, dlnv):
     return lcmc.default_params(num_particles=n, system_density=0.06, system_temperature=T, system_pressure=P,
                                mc_ensemble_type=2, npt_max_dlnV=dlnv, colloid_wall_option=1, colloid_radius=R,
-                               rng_seed=seed, precision_mode=1, cell_capacity=64, **GB_NPT)
+                               rng_seed=seed, precision_mode=1, cell_capacity=0, **GB_NPT)
 
 
 def timed_sweeps(torch, s, k):
