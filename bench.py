@@ -249,9 +249,10 @@ def dilute_start(n, rho0, R, seed):
         np.array([L, L, L])
 
 
-def npt_params(lcmc, n, T, P, R, seed, dlnv, cap=0):
-    """cap: active-cell capacity (0 = chosen from the creation density; systems
-    compressed far beyond it, as the training replicas at P* up to 4 are, need 64)."""
+def npt_params(lcmc, n, T, P, R, seed, dlnv, cap=64):
+    """cap: active-cell capacity of the FP32 kernel (64, the large class, is what
+    the library picks for NPT systems by itself; 48 selects the small class,
+    enough at the density P* = 2 compresses these systems to)."""
     return lcmc.default_params(num_particles=n, system_density=0.06, system_temperature=T, system_pressure=P,
                                mc_ensemble_type=2, npt_max_dlnV=dlnv, colloid_wall_option=1, colloid_radius=R,
                                rng_seed=seed, precision_mode=1, cell_capacity=cap, **GB_NPT)
@@ -279,13 +280,13 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
     # training samples: 16 replicas, compressed from dilute starts, pressures 2..4
     nr, n1 = 16, 32768
     pres = [2.0 + 2.0 * r / (nr - 1) for r in range(nr)]
-    with lcmc.GBSystem([npt_params(lcmc, n1, 0.9, pres[r], 5.0, 200 + r, 0.05, 64) for r in range(nr)]) as s:
+    with lcmc.GBSystem([npt_params(lcmc, n1, 0.9, pres[r], 5.0, 200 + r, 0.05) for r in range(nr)]) as s:
         for r in range(nr):
             st, box = dilute_start(n1, 0.06, 5.0, 300 + r)
             s.upload(*st, box, replica=r)
         s.sweep(600)
         states = [s.download(r) for r in range(nr)]
-    with lcmc.GBSystem([npt_params(lcmc, n1, 0.9, pres[r], 5.0, 400 + r, 0.01, 64) for r in range(nr)]) as s:
+    with lcmc.GBSystem([npt_params(lcmc, n1, 0.9, pres[r], 5.0, 400 + r, 0.01) for r in range(nr)]) as s:
         for r in range(nr):
             s.upload(*states[r][0], states[r][1], replica=r)
         s.sweep(100)
@@ -302,18 +303,18 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
     # the N = 262,144 system: compress from a dilute start, settle at dlnV_max
     # 0.01, then every arm from that one state with one seed
     n = 262144
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05, 64)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05)) as s:
         st, box = dilute_start(n, 0.06, 8.0, 12)
         s.upload(*st, box)
         s.sweep(1000)
         st4, box4 = s.download()
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 13, 0.01, 64)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 13, 0.01)) as s:
         s.upload(*st4, box4)
         s.sweep(1000)
         st4, box4 = s.download()
     arms = {}
     for name in ("plain", "learned", "fp32_screen"):
-        with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01, 64)) as s:
+        with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01)) as s:
             s.upload(*st4, box4)
             if name == "learned":
                 s.set_surrogate(sur)
@@ -370,12 +371,12 @@ def npt_workload(lcmc, torch, n, steps, warmup, screen=False):
     start compressed for 700 sweeps (dlnV_max 0.05), `warmup` sweeps at
     dlnV_max = 0.01, then `steps` timed sweeps; device time per sweep by part."""
     import numpy as np
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05, 48)) as s:
         st, box = dilute_start(n, 0.06, 8.0, 12)
         s.upload(*st, box)
         s.sweep(700)
         st, box = s.download()
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01, 48)) as s:
         s.upload(*st, box)
         s.set_fp32_screen(screen)
         s.sweep(max(3, warmup))

@@ -82,7 +82,9 @@ typedef struct {
     /* added keys */
     uint64_t rng_seed;
     int total_mc_sweeps;
-    int cell_capacity;               /* 0 = automatic */
+    int cell_capacity;               /* active-cell capacity of the FP32 kernel (<= 48: small class, six
+                                        blocks per SM; <= 64: large class); 0 = automatic: NVT from the
+                                        creation density, NPT the large class */
     double npt_max_dlnV;
     int volume_moves_per_sweep;      /* 0 or 1 */
     int precision_mode;              /* LCMC_PREC_FP64 / LCMC_PREC_FP32 */

@@ -522,12 +522,20 @@ static void choose_kernels(lcmc_ctx *c)
         if (kern == 1) {
             c->any_fast = true;
             if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
-            // active-cell capacity: mean occupancy + 12 + 50% (a dense liquid's
-            // cell counts fluctuate far less than that; overflow is flagged)
-            double wcell = rp.L[0] / (double)nc;
-            double mean = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]) * wcell * wcell * wcell;
-            int want = (int)(1.5 * mean + 12.0);
-            if (p.cell_capacity > want) want = p.cell_capacity;
+            // active-cell capacity: the caller's cell_capacity when given; else for
+            // NVT the mean occupancy + 12 + 50% (a dense liquid's cell counts
+            // fluctuate far less than that; overflow is flagged), and for NPT,
+            // whose box may compress far below its creation volume, the large class
+            int want;
+            if (p.cell_capacity > 0) {
+                want = p.cell_capacity;
+            } else if (rp.ensemble == 2) {
+                want = fast_variant(fast_variant_count() - 1).amax;
+            } else {
+                const double wcell = rp.L[0] / (double)nc;
+                const double mean = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]) * wcell * wcell * wcell;
+                want = (int)(1.5 * mean + 12.0);
+            }
             if (want > need_amax) need_amax = want;
         } else {
             c->any_exact = true;

@@ -31,7 +31,7 @@ namespace lcmc {
 
 constexpr int VC_Q = 96;    // queue entries per warp: < 32 pending + 64 from one round of two chunks
 constexpr int VC_CAP = 576; // staged particles per chunk: the own cell and (part of) its forward neighbours
-constexpr int VC_OWN = 128; // own-cell particles
+constexpr int VC_OWN = 256; // own-cell particles (more: F_CELLCAP)
 constexpr int VC_REP = 64;  // replicas whose used cells are enumerated directly (more: every allocated cell)
 
 // replica owning cell slot c (cell ranges are laid out in replica order)

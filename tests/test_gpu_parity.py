@@ -133,12 +133,14 @@ def test_total_energy_vs_oracle(golden, n, R):
         assert abs(e - float(g["plain_E"])) <= 1e-12 * abs(float(g["plain_E"]))
 
 
-@pytest.mark.parametrize("n,sweeps", [(1000, 4), (11000, 2)])
-def test_npt_volume_moves_vs_oracle(n, sweeps):
+@pytest.mark.parametrize("n,sweeps,dmax", [(1000, 4, 0.1), (11000, 2, 0.1), (11000, 2, 1.0)])
+def test_npt_volume_moves_vs_oracle(n, sweeps, dmax):
     """N = 1000: 3 cells per axis (per-particle volume-energy kernel); N = 11000:
-    8 cells per axis (cell kernel for the volume move's energies)."""
+    8 cells per axis (cell kernel for the volume move's energies); with
+    max_displacement 1.0 the cells are 5.5 wide (~51 particles) and a cell's 13
+    forward neighbours exceed one staging chunk (576 particles)."""
     lp, op = params_pair(n, 0.30, 31, precision_mode=0, mc_ensemble_type=2, system_pressure=2.0,
-                         system_temperature=0.9, npt_max_dlnV=0.01)
+                         system_temperature=0.9, npt_max_dlnV=0.01, max_displacement=dmax)
     g_state, box = start_state(lp)
     with lcmc.GBSystem(lp) as s:
         s.set_kernel(0)
