@@ -269,6 +269,27 @@ int lcmc_get_params(lcmc_ctx *ctx, int replica, lcmc_params *out);
  * draws from counters (seed, particle, s); set it to resume a run. */
 int lcmc_set_sweep_counter(lcmc_ctx *ctx, int replica, int64_t sweep);
 
+/* Autotuner (no counterpart in the reference): times `sweeps` sweeps (after
+ * one warm-up sweep) of every candidate configuration -- each FP32 phase-kernel
+ * capacity class the capacity rule allows (the per-block tile of the active
+ * cell: threads, cell capacity, staged candidates per warp, list capacity) and,
+ * for NPT systems with >= 4 cells per axis, the per-cell or the per-particle
+ * kernel for the volume move's exact energies -- and keeps the fastest.  The
+ * state, statistics, sweep counters and last outcomes are restored after every
+ * trial, so the chain continues as if autotune had not run.  With a
+ * cache_path, a choice stored for the same device and workload signature is
+ * applied without timing, and a new choice is appended to the file (one line:
+ * signature, class, volume kernel, ms per sweep).  Call it with history and
+ * volume-sample recording off (LCMC_EINVAL otherwise). */
+typedef struct {
+    int capacity;        /* active-cell capacity of the chosen phase-kernel class */
+    int volume_by_cell;  /* 1: per-cell volume-energy kernel, 0: per-particle */
+    double ms_per_sweep; /* measured time of the chosen configuration */
+    int from_cache;      /* 1: taken from cache_path without timing */
+    int trials;          /* configurations timed */
+} lcmc_tuning;
+int lcmc_autotune(lcmc_ctx *ctx, int sweeps, const char *cache_path, lcmc_tuning *out);
+
 /* The reference's configuration files, byte for byte (host only, no device):
  * fortSphere.1 as esc_fort1 writes it (MCnptColloid.c:3193-3212) and as
  * read_initial_configuration reads it (2786-2831: the first n_max particles of

@@ -57,6 +57,12 @@ class LcmcError(RuntimeError):
 
 _lib = None
 
+class Tuning(C.Structure):
+    """lcmc_tuning."""
+    _fields_ = [("capacity", C.c_int), ("volume_by_cell", C.c_int), ("ms_per_sweep", C.c_double),
+                ("from_cache", C.c_int), ("trials", C.c_int)]
+
+
 EXPORTS = {
     "lcmc_params_defaults": ([C.POINTER(Params)], C.c_int),
     "lcmc_params_load": ([C.c_char_p, C.POINTER(Params)], C.c_int),
@@ -99,6 +105,7 @@ EXPORTS = {
     "lcmc_set_adaptive_step": ([C.c_void_p, C.c_int], C.c_int),
     "lcmc_get_step": ([C.c_void_p, C.c_int, DP, DP], C.c_int),
     "lcmc_set_sweep_counter": ([C.c_void_p, C.c_int, C.c_int64], C.c_int),
+    "lcmc_autotune": ([C.c_void_p, C.c_int, C.c_char_p, C.POINTER(Tuning)], C.c_int),
     "lcmc_write_fort1": ([C.c_char_p, C.c_int, DP, DP, DP, DP, DP, DP, DP, C.c_double], C.c_int),
     "lcmc_read_fort1": ([C.c_char_p, C.c_int, DP, DP, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_int)], C.c_int),
     "lcmc_write_trajectory": ([C.c_char_p, C.c_int, C.c_int, DP, DP, DP, DP, DP, DP, DP], C.c_int),

@@ -70,6 +70,7 @@ struct lcmc_ctx {
     // kernels
     int kernel_override = -1;
     int fast_variant = 0;
+    int need_amax = 0; // active-cell capacity the capacity rule asks for
     int grid_elem = 0, grid_exact = 0, grid_fast = 0, grid_energy = 0, grid_screen = 0;
     bool any_fast = false, any_exact = false, any_npt = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -543,6 +544,7 @@ static void choose_kernels(lcmc_ctx *c)
         if (rp.ensemble == 2) c->any_npt = true;
         spec21 = spec21 && p.gb_mu_exponent == 2.0 && p.gb_nu_exponent == 1.0 && p.gb_sigma_sidetoside == 1.0;
     }
+    c->need_amax = need_amax;
     c->fast_variant = 2 * (need_amax > fast_variant(0).amax ? 1 : 0) + (spec21 ? 1 : 0);
 }
 
@@ -584,6 +586,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
         rp.dlnv_max = rp.ensemble == 2 && p.volume_moves_per_sweep > 0 ? p.npt_max_dlnV : 0.0;
         rp.wmin = min_cell_width(p);
         rp.d_cap = (double)p.max_displacement;
+        rp.vol_cells = 1;
         rp.min_thick = (double)(float)std::min(p.gb_sigma_sidetoside * p.gb_kappa, p.gb_sigma_sidetoside);
         seed_key(p.rng_seed, rp.key);
         make_consts(p, rp.k);
@@ -1290,5 +1293,217 @@ extern "C" int lcmc_order_parameter(lcmc_ctx *ctx, int replica, double Q[6], dou
         director[1] = V[1][im];
         director[2] = V[2][im];
     }
+    return LCMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner (no reference counterpart): measured choice of the FP32 phase
+// kernel's capacity class and of the kernel for the volume move's energies
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct TuneChoice {
+    int variant_class; // index into the phase-kernel capacity classes
+    int vol_cells;     // 1: per-cell volume-energy kernel, 0: per-particle kernel
+};
+
+// The workload signature a cached choice is valid for: device, replica layout
+// and every replica's size, ensemble, kernel, grid capacity and screen.
+std::string tune_key(const lcmc_ctx *c)
+{
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) prop.name[0] = 0;
+    std::string k = std::string(prop.name) + "|sms=" + std::to_string(c->sms) + "|R=" + std::to_string(c->R);
+    for (int r = 0; r < c->R; r++) {
+        const Replica &rp = c->rep[r];
+        const lcmc_params &p = c->params[r];
+        char b[160];
+        snprintf(b, sizeof(b), "|%d,%d,%d,%d,%d,%.3g,%d", rp.n, rp.ensemble, rp.kernel, rp.nc_max, rp.da_kind,
+                 p.system_density, p.cell_capacity);
+        k += b;
+    }
+    for (char &ch : k)
+        if (ch == '\t' || ch == '\n') ch = ' ';
+    return k;
+}
+
+bool tune_cache_read(const char *path, const std::string &key, TuneChoice &ch, double &ms)
+{
+    if (!path) return false;
+    FILE *f = fopen(path, "r");
+    if (!f) return false;
+    char line[8192];
+    bool found = false;
+    while (fgets(line, sizeof(line), f)) {
+        char *tab = strchr(line, '\t');
+        if (!tab) continue;
+        *tab = 0;
+        if (key != line) continue;
+        int a = 0, b = 0;
+        double m = 0.0;
+        if (sscanf(tab + 1, "%d\t%d\t%lf", &a, &b, &m) == 3 && a >= 0 && a < fast_variant_count() && (b == 0 || b == 1)) {
+            ch.variant_class = a;
+            ch.vol_cells = b;
+            ms = m;
+            found = true; // the last entry for a key wins
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+void tune_cache_append(const char *path, const std::string &key, const TuneChoice &ch, double ms)
+{
+    if (!path) return;
+    FILE *f = fopen(path, "a");
+    if (!f) return;
+    fprintf(f, "%s\t%d\t%d\t%.6f\n", key.c_str(), ch.variant_class, ch.vol_cells, ms);
+    fclose(f);
+}
+
+} // namespace
+
+static int apply_tuning(lcmc_ctx *c, const TuneChoice &ch)
+{
+    c->fast_variant = 2 * ch.variant_class + (c->fast_variant & 1);
+    c->grid_fast = fast_blocks_per_sm(c->fast_variant) * c->sms;
+    for (int r = 0; r < c->R; r++) {
+        Replica &rp = c->rep[r];
+        rp.vol_cells = ch.vol_cells;
+        CUDA_TRY(c, cudaMemcpyAsync((char *)c->d_rep + sizeof(Replica) * r + offsetof(Replica, vol_cells), &rp.vol_cells,
+                                    sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    invalidate_graphs(c);
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_autotune(lcmc_ctx *ctx, int sweeps, const char *cache_path, lcmc_tuning *out)
+{
+    if (!ctx || sweeps < 1) return LCMC_EINVAL;
+    for (int r = 0; r < ctx->R; r++)
+        if (!ctx->uploaded[r]) return set_err(ctx, LCMC_EINVAL, "replica has no configuration (upload or init first)");
+    if (ctx->hist_cap > 0 || ctx->rec_cap > 0)
+        return set_err(ctx, LCMC_EINVAL, "autotune before recording history or volume samples");
+    const std::string key = tune_key(ctx);
+    TuneChoice best{ctx->fast_variant >> 1, 1};
+    double best_ms = 0.0;
+    lcmc_tuning res;
+    memset(&res, 0, sizeof(res));
+    if (tune_cache_read(cache_path, key, best, best_ms)) {
+        int rc = apply_tuning(ctx, best);
+        if (rc) return rc;
+        res.from_cache = 1;
+    } else {
+        // candidates: every capacity class the capacity rule allows, each volume-energy kernel that applies
+        std::vector<TuneChoice> cand;
+        bool npt4 = false; // an NPT replica on the per-cell volume kernel's grid (>= 4 cells per axis)
+        for (int r = 0; r < ctx->R; r++)
+            npt4 = npt4 || (ctx->rep[r].ensemble == 2 && grid_dim_host(ctx->rep[r].L[0], ctx->rep[r].wmin) >= 4);
+        for (int v = 0; v < fast_variant_count(); v++) {
+            if (!ctx->any_fast && v != (ctx->fast_variant >> 1)) continue;
+            // classes below the rule's capacity are not tried (the largest always is)
+            if (ctx->any_fast && fast_variant(v).amax < ctx->need_amax && v != fast_variant_count() - 1) continue;
+            cand.push_back({v, 1});
+            if (npt4) cand.push_back({v, 0});
+        }
+        // snapshot: the current state buffer, ids, replica table, statistics, outcomes
+        const int cur = ctx->cur;
+        const size_t n = (size_t)ctx->ntot;
+        double *sx = nullptr;
+        int *sid = nullptr;
+        Replica *srep = nullptr;
+        DevStats *sst = nullptr;
+        unsigned char *sout = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        auto release = [&]() {
+            cudaFree(sx);
+            cudaFree(sid);
+            cudaFree(srep);
+            cudaFree(sst);
+            cudaFree(sout);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        };
+        if (cudaMalloc(&sx, sizeof(double) * 6 * n) != cudaSuccess || cudaMalloc(&sid, sizeof(int) * n) != cudaSuccess ||
+            cudaMalloc(&srep, sizeof(Replica) * ctx->R) != cudaSuccess ||
+            cudaMalloc(&sst, sizeof(DevStats) * ctx->R) != cudaSuccess || cudaMalloc(&sout, n) != cudaSuccess ||
+            cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+            release();
+            cudaGetLastError();
+            return set_err(ctx, LCMC_ENOMEM, "autotune snapshot");
+        }
+        auto copy_state = [&](bool save) -> cudaError_t {
+            cudaError_t e = cudaSuccess;
+            for (int k = 0; k < 6 && e == cudaSuccess; k++)
+                e = save ? cudaMemcpyAsync(sx + k * n, ctx->d_x[cur][k], sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                           ctx->stream)
+                         : cudaMemcpyAsync(ctx->d_x[cur][k], sx + k * n, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                           ctx->stream);
+            if (e == cudaSuccess)
+                e = save ? cudaMemcpyAsync(sid, ctx->d_id[cur], sizeof(int) * n, cudaMemcpyDeviceToDevice, ctx->stream)
+                         : cudaMemcpyAsync(ctx->d_id[cur], sid, sizeof(int) * n, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e == cudaSuccess)
+                e = save ? cudaMemcpyAsync(srep, ctx->d_rep, sizeof(Replica) * ctx->R, cudaMemcpyDeviceToDevice,
+                                           ctx->stream)
+                         : cudaMemcpyAsync(ctx->d_rep, srep, sizeof(Replica) * ctx->R, cudaMemcpyDeviceToDevice,
+                                           ctx->stream);
+            if (e == cudaSuccess)
+                e = save ? cudaMemcpyAsync(sst, ctx->d_stats, sizeof(DevStats) * ctx->R, cudaMemcpyDeviceToDevice,
+                                           ctx->stream)
+                         : cudaMemcpyAsync(ctx->d_stats, sst, sizeof(DevStats) * ctx->R, cudaMemcpyDeviceToDevice,
+                                           ctx->stream);
+            if (e == cudaSuccess)
+                e = save ? cudaMemcpyAsync(sout, ctx->d_outcome, n, cudaMemcpyDeviceToDevice, ctx->stream)
+                         : cudaMemcpyAsync(ctx->d_outcome, sout, n, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (!save) ctx->cur = cur;
+            return e;
+        };
+        if (copy_state(true) != cudaSuccess) {
+            release();
+            return set_err(ctx, LCMC_ECUDA, "autotune snapshot");
+        }
+        best_ms = -1.0;
+        int rc = LCMC_OK;
+        for (const TuneChoice &ch : cand) {
+            rc = apply_tuning(ctx, ch);
+            if (rc) break;
+            rc = lcmc_sweep(ctx, 1); // warm-up: captures the graph
+            double ms = -1.0;
+            if (rc == LCMC_OK) {
+                cudaEventRecord(e0, ctx->stream);
+                rc = lcmc_sweep(ctx, sweeps);
+                cudaEventRecord(e1, ctx->stream);
+                float t = 0.0f;
+                if (rc == LCMC_OK && cudaEventSynchronize(e1) == cudaSuccess &&
+                    cudaEventElapsedTime(&t, e0, e1) == cudaSuccess)
+                    ms = t / sweeps;
+            }
+            res.trials++;
+            if (copy_state(false) != cudaSuccess) {
+                release();
+                return set_err(ctx, LCMC_ECUDA, "autotune restore");
+            }
+            if (rc == LCMC_ECELLCAP) rc = LCMC_OK; // this class is too small for the configuration
+            if (rc) break;
+            if (ms > 0.0 && (best_ms < 0.0 || ms < best_ms)) {
+                best_ms = ms;
+                best = ch;
+            }
+        }
+        release();
+        if (rc) return rc;
+        if (best_ms < 0.0) return set_err(ctx, LCMC_ECELLCAP, "no candidate ran");
+        rc = apply_tuning(ctx, best);
+        if (rc) return rc;
+        tune_cache_append(cache_path, key, best, best_ms);
+    }
+    res.capacity = fast_variant(best.variant_class).amax;
+    res.volume_by_cell = best.vol_cells;
+    res.ms_per_sweep = best_ms;
+    if (out) *out = res;
+    ctx->err.clear();
     return LCMC_OK;
 }

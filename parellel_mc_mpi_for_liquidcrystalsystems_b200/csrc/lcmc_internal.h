@@ -49,6 +49,7 @@ struct Replica {
     int vol_stage1;    // this sweep: 0 rejected by the screen, 1 no screen, 2 passed the screen
     double da_scale;   // surrogate output -> dU / N
     double vol_dU_sur; // surrogate dU of this sweep's move
+    int vol_cells;     // 1: the volume move's exact energies by the per-cell kernel (>= 4 cells per axis)
 };
 
 constexpr int LCMC_FEAT = 8 * 512 + 1; // surrogate input: 8 channels x 8^3 cells + delta ln V

@@ -53,7 +53,7 @@ __device__ __forceinline__ bool volume_cells_serves(const Replica &p)
     if (p.ensemble != 2) return false;
     if (!EXACT) return p.da_kind == 2 && p.use_fast;
     if (p.da_on && !p.vol_stage1) return false; // screened out: no exact recompute
-    return p.nc[0] >= 4 && p.nc[1] >= 4 && p.nc[2] >= 4;
+    return p.vol_cells && p.nc[0] >= 4 && p.nc[1] >= 4 && p.nc[2] >= 4;
 }
 
 template <bool EXACT>

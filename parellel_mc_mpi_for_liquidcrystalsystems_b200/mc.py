@@ -145,6 +145,15 @@ class GBSystem:
         d["box"] = list(s.box)
         return d
 
+    def autotune(self, sweeps=3, cache=None):
+        """Time every candidate kernel configuration over `sweeps` sweeps and
+        keep the fastest (lcmc_autotune); the chain continues as if it had not
+        run.  `cache`: file of earlier choices, read and appended."""
+        t = _lib.Tuning()
+        self._check(lib().lcmc_autotune(self._h, int(sweeps), str(cache).encode() if cache else None, C.byref(t)))
+        return {"capacity": t.capacity, "volume_by_cell": bool(t.volume_by_cell), "ms_per_sweep": t.ms_per_sweep,
+                "from_cache": bool(t.from_cache), "trials": t.trials}
+
     def tot_ene(self, replica=0):
         """tot_ene (MCnptColloid.c:1598-1622): FP64 recompute of the total energy."""
         e = C.c_double()

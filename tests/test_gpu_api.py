@@ -163,3 +163,64 @@ def test_adaptive_step_follows_the_reference_rule():
         s.set_adaptive_step(False)
         s.sweep(5)
         assert s.step() == (d, a)
+
+
+def test_autotune_keeps_the_chain(tmp_path):
+    """lcmc_autotune times both phase-kernel capacity classes (11,000 rods, 8
+    cells per axis, ~22 per cell) and restores everything after each trial: the
+    chain continues bit for bit as an untuned run's.  A second context with the
+    same workload takes the choice from the cache file without timing."""
+    p = lcmc.default_params(num_particles=11000, system_density=0.30, rng_seed=17, precision_mode=1, **COMMON)
+    cache = tmp_path / "tune.tsv"
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(3)
+        before, _ = s.download()
+        t = s.autotune(2, cache)
+        assert t["trials"] == 2 and not t["from_cache"] and t["ms_per_sweep"] > 0.0
+        assert t["capacity"] in (48, 64)
+        after, _ = s.download()
+        for u, v in zip(before, after):
+            assert np.array_equal(bits(u), bits(v))
+        assert s.stats()["sweeps"] == 3
+        s.sweep(3)
+        tuned, box1 = s.download()
+        st1 = s.stats()
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(6)
+        plain, box2 = s.download()
+        st2 = s.stats()
+    for u, v in zip(tuned, plain):
+        assert np.array_equal(bits(u), bits(v))
+    assert st1["attempted"] == st2["attempted"] == 6 * 11000
+    assert st1["accepted"] == st2["accepted"] and st1["energy"] == st2["energy"]
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        t2 = s.autotune(2, cache)
+        assert t2["from_cache"] and t2["trials"] == 0 and t2["capacity"] == t["capacity"]
+        s.sweep(1)
+
+
+def test_autotune_npt_volume_kernels():
+    """For an NPT system with >= 4 cells per axis both kernels for the volume
+    move's energies are timed; state and statistics are untouched."""
+    p = lcmc.default_params(num_particles=11000, system_density=0.30, rng_seed=23, precision_mode=1,
+                            mc_ensemble_type=2, system_pressure=2.0, system_temperature=1.2, npt_max_dlnV=0.01,
+                            **COMMON)
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(2)
+        before, box0 = s.download()
+        st0 = s.stats()
+        t = s.autotune(1)
+        assert t["trials"] == 2 and t["capacity"] == 64
+        after, box1 = s.download()
+        for u, v in zip(before, after):
+            assert np.array_equal(bits(u), bits(v))
+        assert np.array_equal(bits(box0), bits(box1))
+        st1 = s.stats()
+        assert (st1["sweeps"], st1["volume_attempted"], st1["energy"]) == (st0["sweeps"], st0["volume_attempted"],
+                                                                          st0["energy"])
+        s.sweep(2)
+        assert s.stats()["volume_attempted"] == st0["volume_attempted"] + 2
