@@ -398,6 +398,26 @@ def npt_workload(lcmc, torch, n, steps, warmup, screen=False):
 
 
 # ---------------------------------------------------------------------------
+# ranks: the job's time is the slowest rank's; value = all ranks' units / that
+# ---------------------------------------------------------------------------
+def max_over_ranks(dist, x, device="cuda"):
+    """Largest of the ranks' values of x, on every rank (x itself without a
+    process group)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, seconds):
+    """Whole-job throughput of a weak-scaling run: every rank processed
+    units_per_rank in a job that took `seconds` (the max over ranks)."""
+    return units_per_rank * world / seconds
+
+
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -478,15 +498,12 @@ def main():
             step_ms.append(a.elapsed_time(b))
             phase_ms.append(s.last_sweep_timing()[1])
     torch.cuda.synchronize()
-    total_ms = sum(step_ms)
+    total_ms = max_over_ranks(dist, sum(step_ms))
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     st1 = s.stats()
     attempted = st1["attempted"] - st0["attempted"]
-    value = N_PART * args.steps * world / (total_ms * 1e-3)
+    value = job_rate(N_PART * args.steps, world, total_ms * 1e-3)
 
     # roofline of the colour-phase kernel: algorithmic flops per attempt
     # 2 (8 C + 61 P): C = 27-cell stencil candidates, P = in-cutoff pairs per state
@@ -514,12 +531,8 @@ def main():
         s.sweep(1)
         _, box = s.download(out=hv)
         energy = s.stats()["energy"]
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = N_PART * args.e2e_steps * world / e2e_s
+    e2e_s = max_over_ranks(dist, time.perf_counter() - t0)
+    e2e = job_rate(N_PART * args.e2e_steps, world, e2e_s)
     kps = s.kernels_per_sweep()
     st = s.stats()
     e_exact = s.tot_ene()  # FP64 recompute of the final state (outside the timed region)
