@@ -476,9 +476,10 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
             // by fixed-point rounds in parallel.  Each round recomputes every
             // dE_k from the current guess of the earlier decisions, adding the
             // terms in increasing m exactly as a sequential scan would; after
-            // round r the first r decisions are final, and a round that changes
-            // no decision has reached the unique solution (usually round 2 or
-            // 3), so the decisions and dE_k equal the sequential scan's bits.
+            // pass r the first r decisions are final, and a pass that changes
+            // no decision has reached the unique solution (usually the second
+            // or third pass), so the decisions and dE_k equal the sequential
+            // scan's bits.
             const double beta = p.k.beta;
             const bool v0 = lane < na, v1 = lane + 32 < na;
             const unsigned hd0 = __ballot_sync(0xffffffffu, v0 && sm.hard[lane]);
