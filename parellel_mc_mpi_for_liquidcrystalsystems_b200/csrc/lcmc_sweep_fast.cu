@@ -8,21 +8,18 @@
 // gather, k_gather).  So for every particle k the energy against the 26 static
 // cells, old and new, is independent of the other attempts:
 //
-//   dE_k = [S_new(k) - S_old(k)]                            static cells
-//        + sum_{m != k} [phi(n_k, o_m) - phi(o_k, o_m)]     in-cell, old states
-//        + sum_{m < k, m accepted} c(k, m)                  in-cell corrections
+//   dE_k = [S_new(k) - S_old(k)]                               static cells
+//        + sum_{m > k} [phi(n_k, o_m) - phi(o_k, o_m)]          later in-cell partners
+//        + sum_{m < k} [phi(n_k, n_m) - phi(o_k, n_m)]  if m was accepted,
+//                      [phi(n_k, o_m) - phi(o_k, o_m)]  if not  earlier partners
 //        + U_coll(n_k) - U_coll(o_k)
-//   c(k, m) = [phi(n_k, n_m) - phi(o_k, n_m)] - [phi(n_k, o_m) - phi(o_k, o_m)]
 //
-// The scan adds, for every earlier partner m, either phi(n_k, n_m) - phi(o_k, n_m)
-// (m accepted) or phi(n_k, o_m) - phi(o_k, o_m) (m rejected), never one and then
-// the correction: a near-overlap term of 1e20 or more that would cancel must not
-// pass through the FP64 sum, whose rounding at that size (1e4 and up) would
-// swamp dE_k.
-//
-// which is exactly E_new - E_old of attempt_monte_carlo_move (MCnptColloid.c:
-// 2491-2563) for the sequential in-cell order (ascending id).  Only the short
-// scan over the accept decisions is sequential.
+// Each earlier partner contributes exactly one of its two terms, never one and
+// then a correction: a near-overlap term of 1e20 or more that would cancel must
+// not pass through the FP64 sum, whose rounding at that size (1e4 and up) would
+// swamp dE_k.  This is exactly E_new - E_old of attempt_monte_carlo_move
+// (MCnptColloid.c:2491-2563) for the sequential in-cell order (ascending id);
+// only the decisions depend on each other, through a triangular system.
 //
 // Phases per cell:
 //   1 stencil  27 cells (>= 4 cells per axis, no duplicates)
@@ -47,8 +44,8 @@
 //   5 sums     warp 0, thread per particle: static + colloid + later in-cell
 //              partners (per-particle trial data was prefetched into shared
 //              memory in step 2)
-//   6 decide   warp 0: Metropolis decisions in id order (fixed-point rounds of
-//              the triangular system the sequential order defines)
+//   6 decide   warp 0: Metropolis decisions in id order (fixed-point passes
+//              over the triangular system the sequential order defines)
 //   7 write    accepted trial states to the FP64 master arrays
 #include <cuda_runtime.h>
 
