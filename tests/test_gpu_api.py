@@ -224,3 +224,42 @@ def test_autotune_npt_volume_kernels():
                                                                           st0["energy"])
         s.sweep(2)
         assert s.stats()["volume_attempted"] == st0["volume_attempted"] + 2
+
+
+@pytest.mark.parametrize("bad,code", [
+    (dict(num_particles=0), _lib.EINVAL),
+    (dict(system_density=-0.3), _lib.EINVAL),
+    (dict(system_temperature=0.0), _lib.EINVAL),
+    (dict(num_particles=8), _lib.EBOX),  # L = 3 < 2 rc
+])
+def test_create_rejects_bad_parameters(bad, code):
+    """Invalid sizes come back as status codes (the reference exits or runs on),
+    for a single system and for a batch holding one bad replica; a good
+    context still works afterwards."""
+    good = lcmc.default_params(num_particles=2000, system_density=0.30, rng_seed=1, **COMMON)
+    kw = dict(COMMON, num_particles=2000, system_density=0.30, rng_seed=1)
+    kw.update(bad)
+    p = lcmc.default_params(**kw)
+    for arg in (p, [good, p]):
+        with pytest.raises(lcmc.LcmcError) as ei:
+            lcmc.GBSystem(arg)
+        assert ei.value.code == code
+    with lcmc.GBSystem(good) as s:
+        s.get_initial_config()
+        s.sweep(1)
+        assert s.stats()["attempted"] == 2000
+
+
+def test_sweep_before_upload_and_bad_replica_index():
+    p = lcmc.default_params(num_particles=2000, system_density=0.30, rng_seed=2, **COMMON)
+    with lcmc.GBSystem([p, p]) as s:
+        s.get_initial_config(0)
+        with pytest.raises(lcmc.LcmcError) as ei:
+            s.sweep(1)  # replica 1 holds no configuration
+        assert ei.value.code == _lib.EINVAL
+        with pytest.raises(lcmc.LcmcError) as ei:
+            s.stats(2)
+        assert ei.value.code == _lib.EINVAL
+        s.get_initial_config(1)
+        s.sweep(1)
+        assert s.stats(1)["attempted"] == 2000
