@@ -81,7 +81,7 @@ typedef struct {
     double colloid_radius;
     /* added keys */
     uint64_t rng_seed;
-    int total_mc_sweeps;
+    int total_mc_sweeps;             /* sweeps of a run_simulation driver run; 0 = ceil(total_mc_cycles / num_particles) */
     int cell_capacity;               /* active-cell capacity of the FP32 kernel (<= 48: small class, six
                                         blocks per SM; <= 64: large class); 0 = automatic: NVT from the
                                         creation density, NPT the large class */

@@ -30,7 +30,7 @@ int lco_params_defaults(lco_params *p)
 {
     memset(p, 0, sizeof(*p));
     p->rng_seed = 12345u;
-    p->total_mc_sweeps = 100;
+    p->total_mc_sweeps = 0;
     p->cell_capacity = 0;
     p->npt_max_dlnV = 0.01;
     p->volume_moves_per_sweep = 1;

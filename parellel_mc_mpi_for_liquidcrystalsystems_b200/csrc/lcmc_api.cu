@@ -167,7 +167,7 @@ extern "C" int lcmc_params_defaults(lcmc_params *p)
     p->colloid_interaction_amplitude = 1.5;
     p->colloid_radius = 0.0;
     p->rng_seed = 12345u;
-    p->total_mc_sweeps = 100;
+    p->total_mc_sweeps = 0;
     p->cell_capacity = 0;
     p->npt_max_dlnV = 0.01;
     p->volume_moves_per_sweep = 1;

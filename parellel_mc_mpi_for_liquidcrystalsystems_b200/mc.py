@@ -294,3 +294,82 @@ def run(params, n_sweeps, stats_interval=10, callback=None):
                 callback(rec)
         n = max(sums["n"], 1)
         return {"E_per_N": sums["E"] / n, "rho": sums["rho"] / n, "P2": sums["P2"] / n, "stats": s.stats()}
+
+
+def run_simulation(params, out_dir=".", adaptive=False, histogram=True, log=None):
+    """The reference's main cycle loop (MCnptColloid.c:887-1061) over this
+    library, at sweep granularity: one sweep is num_particles attempts, where a
+    reference cycle is a single attempt, so intervals given in cycles become
+    ceil(interval / N) sweeps, and the run lasts total_mc_sweeps sweeps (or
+    ceil(total_mc_cycles / N) when that key is 0).
+
+    * start: initial_configuration_type 0 reads out_dir/fortSphere.1
+      (read_initial_configuration; exactly, when its .lcmc sidecar is there),
+      2 the lattice; 1 (random placement) is not provided;
+    * every configuration_save_interval: a status line to `log`
+      (print_intermedio), a snapshot appended to Configuraciones.dat
+      (print_Trayectoria) and fortSphere.1 rewritten (backup_restart_file, with
+      the exact sidecar);
+    * every statistics_print_interval: P2 and the running averages of E/N, rho
+      and P2 (compute_liquid_crystal_order_parameters, update_running_averages);
+    * `adaptive`: the step-size controller (the reference always runs it; here
+      it is for equilibration and off by default);
+    * at the end: qmga_mcnvtGB.cnf (print_Qmga), Histograma_Movimientos.dat
+      (accepted moves per particle id) and fortSphere.1 (esc_fort1).
+
+    `params`: lcmc_params or the path of a parametersFile.txt.  Returns the
+    averages and the final statistics."""
+    import math
+    import os
+    if not isinstance(params, Params):
+        params = load_initial_conditions(params)
+    n = params.num_particles
+    sweeps = params.total_mc_sweeps if params.total_mc_sweeps > 0 else math.ceil(params.total_mc_cycles / n)
+    save_every = max(1, math.ceil(params.configuration_save_interval / n))
+    stats_every = max(1, math.ceil(params.statistics_print_interval / n))
+    os.makedirs(out_dir, exist_ok=True)
+    path = lambda name: os.path.join(out_dir, name)  # noqa: E731
+    avg = {"E": 0.0, "rho": 0.0, "P2": 0.0, "n": 0}
+    hist = np.zeros(n, dtype=np.int64)
+    with GBSystem(params) as s:
+        if params.initial_configuration_type == 0:
+            s.load_restart(path("fortSphere.1"))
+        elif params.initial_configuration_type == 2:
+            s.get_initial_config()
+        else:
+            raise LcmcError(_lib.EPARAM, "initial_configuration_type 1 (random placement) is not provided")
+        if adaptive:
+            s.set_adaptive_step(True)
+        first = True
+        P2 = 0.0
+        for sweep in range(1, sweeps + 1):
+            s.sweep(1)
+            if histogram:
+                hist += s.outcomes() == 1
+            if sweep % stats_every == 0:
+                st = s.stats()
+                _, P2, _ = s.compute_liquid_crystal_order_parameters()
+                V = st["box"][0] * st["box"][1] * st["box"][2]
+                avg["E"] += st["energy"] / n
+                avg["rho"] += n / V
+                avg["P2"] += P2
+                avg["n"] += 1
+            if sweep % save_every == 0:
+                st = s.stats()
+                if log:
+                    k = max(avg["n"], 1)
+                    log(f"sweep {sweep}: E/N {st['energy'] / n:.6f} <E/N> {avg['E'] / k:.6f} P2 {P2:.4f} "
+                        f"<P2> {avg['P2'] / k:.4f} <rho> {avg['rho'] / k:.5f} "
+                        f"acceptance {st['accepted'] / max(st['attempted'], 1):.4f}")
+                s.print_Trayectoria(path("Configuraciones.dat"), append=not first)
+                first = False
+                s.save_restart(path("fortSphere.1"))
+        s.print_Qmga(path("qmga_mcnvtGB.cnf"))
+        if histogram:
+            with open(path("Histograma_Movimientos.dat"), "w") as f:
+                for i, h in enumerate(hist):
+                    f.write(f"{i}       {h}\n")
+        s.save_restart(path("fortSphere.1"))
+        k = max(avg["n"], 1)
+        return {"sweeps": sweeps, "E_per_N": avg["E"] / k, "rho": avg["rho"] / k, "P2": avg["P2"] / k,
+                "stats": s.stats()}
