@@ -397,6 +397,43 @@ def npt_workload(lcmc, torch, n, steps, warmup, screen=False):
                 "kernels_per_sweep": s.kernels_per_sweep()}
 
 
+def port_cpu(n_part, seconds=8.0, threads=None):
+    """The same checkerboard algorithm on the host cores: the oracle's FP64
+    cell-list sweep (oracle/lcmc_oracle.c, lco_sweep_parallel) with each
+    colour's active cells shared among OpenMP threads, on the workload's own
+    lattice start, whole sweeps until `seconds` have passed (at least one)."""
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import numpy as np
+
+    import oracle_ctypes as oc
+    threads = threads or os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    try:
+        oc.omp_lib()
+    except OSError as e:
+        return None, f"oracle OpenMP build not loadable: {e}"
+    *state, box = oc.init_lattice(n=n_part, rho=0.32, seed=1234, cone=20.0)
+    state = [np.ascontiguousarray(x) for x in state]
+    p = oc.params(num_particles=n_part, system_density=0.32, system_temperature=0.8, max_displacement=0.1,
+                  max_rotation=0.1, cutoff_radius=4.0, rng_seed=1234, init_orientation_cone_deg=20.0)
+    consts = oc.Consts()
+    oc.omp_lib().lco_consts_from_params(C.byref(p), oc.ARITH_CANONICAL, C.byref(consts))
+    key = (C.c_uint32 * 2)()
+    oc.omp_lib().lco_key(1234, 0, key)
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        oc.sweep_parallel(consts, key, done, state, box)
+        done += 1
+        dt = time.perf_counter() - t0
+        if dt >= seconds:
+            break
+    return {"value": n_part * done / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{done} sweep(s) of the oracle's FP64 checkerboard (cell lists, lco_sweep_parallel) at "
+                      f"N={n_part} from the workload's lattice start in {dt:.1f} s, OpenMP threads={threads}",
+            "seconds": dt}, None
+
+
 # ---------------------------------------------------------------------------
 # ranks: the job's time is the slowest rank's; value = all ranks' units / that
 # ---------------------------------------------------------------------------
@@ -426,6 +463,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--port-seconds", type=float, default=8.0,
+                    help="host time for the checkerboard port baseline (0 skips it)")
     ap.add_argument("--da-sweeps", type=int, default=4000,
                     help="sweeps per arm of the NPT delayed-acceptance measurement (0 skips it)")
     ap.add_argument("--da-train-sweeps", type=int, default=400)
@@ -547,6 +586,8 @@ def main():
     sgemm = fp32_peak_tflops(torch)
     nominal = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     cpu, why = reference_cpu(N_PART, seconds=args.cpu_seconds) if world == 1 else (None, "rank 0 of N>1")
+    port, port_why = port_cpu(N_PART, seconds=args.port_seconds) if world == 1 and args.port_seconds > 0 \
+        else (None, "not run")
     clocks = clk.summary()
     traffic = kernel_traffic()
     npt = None
@@ -574,6 +615,7 @@ def main():
                      "in_cutoff_pairs_per_attempt_old_plus_new": P2_att, "avg_launch_ms": avg_launch_ms,
                      "phase_share_of_step": statistics.mean(phase_ms) / (total_ms / args.steps)},
         "cpu_baseline": cpu if cpu else {"unavailable": why},
+        "cpu_port": port if port else {"unavailable": port_why},
         "acceptance": (st["accepted"] / max(st["attempted"], 1)),
         # the lattice start holds overlapping rods (pair terms up to ~1e36), so the
         # running FP64 energy carries their rounding; the recompute is the state's energy

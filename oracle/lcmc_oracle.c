@@ -754,6 +754,78 @@ static double butterfly32(double part[32])
  * with the colloid term added only when colloid_wall_option == 1 and Philox
  * draws in place of rand().  The sums over the stencil use the canonical
  * 32-way order of butterfly32. */
+/* One trial move of particle k against the staged stencil particles slots[0..S)
+ * (attempt_monte_carlo_move, MCnptColloid.c:2474-2598, with the checkerboard's
+ * pick and Philox draws): 0 rejected, 1 accepted (state written, *de set),
+ * 2 hard-core reject. */
+static int attempt_move(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int k, const int *slots, int S,
+                        double *px, double *py, double *pz, double *ox, double *oy, double *oz, const double box[3],
+                        double *de_out)
+{
+    uint32_t rnd[4];
+    philox_at(key, (uint32_t)k, sweep, TAG_MOVE, rnd);
+    double ro[3] = {px[k], py[k], pz[k]}, eo[3] = {ox[k], oy[k], oz[k]};
+    double rn[3];
+    rn[0] = ro[0] + c->max_disp * (lco_u01(rnd[0]) - 0.5);
+    rn[1] = ro[1] + c->max_disp * (lco_u01(rnd[1]) - 0.5);
+    rn[2] = ro[2] + c->max_disp * (lco_u01(rnd[2]) - 0.5);
+    lco_apply_pbc(&rn[0], &rn[1], &rn[2], box);
+    double ddx, ddy, ddz;
+    double rc2c = lco_distance_sq(rn[0], rn[1], rn[2], 0.5 * box[0], 0.5 * box[1], 0.5 * box[2], box, &ddx, &ddy,
+                                  &ddz);
+    if (!(rc2c > c->coll_R * c->coll_R)) return 2;
+    double v[3];
+    lco_sphere_point(key, (uint32_t)k, sweep, v);
+    double en[3];
+    en[0] = c->max_rot * v[0] + eo[0];
+    en[1] = c->max_rot * v[1] + eo[1];
+    en[2] = c->max_rot * v[2] + eo[2];
+    double norm2 = en[0] * en[0] + en[1] * en[1] + en[2] * en[2];
+    if (norm2 <= 1e-12) {
+        en[0] = eo[0]; en[1] = eo[1]; en[2] = eo[2];
+    } else {
+        double nr = sqrt(norm2);
+        en[0] /= nr; en[1] /= nr; en[2] /= nr;
+    }
+    double po[32], pn[32];
+    memset(po, 0, sizeof(po));
+    memset(pn, 0, sizeof(pn));
+    for (int q = 0; q < S; q++) {
+        int j = slots[q];
+        if (j == k) continue;
+        double rj[3] = {px[j], py[j], pz[j]}, ej[3] = {ox[j], oy[j], oz[j]};
+        int in;
+        double vo = lco_pair(c, ro, eo, rj, ej, box, &in);
+        if (in) po[q & 31] += vo;
+        double vn = lco_pair(c, rn, en, rj, ej, box, &in);
+        if (in) pn[q & 31] += vn;
+    }
+    double Eo = butterfly32(po), En = butterfly32(pn);
+    if (c->coll_on) {
+        Eo = Eo + lco_colloid_rod(c, ro, eo, box);
+        En = En + lco_colloid_rod(c, rn, en, box);
+    }
+    double de = En - Eo;
+    int acc = (de <= 0.0) || (lco_log(lco_u01(rnd[3])) <= -c->beta * de);
+    if (acc) {
+        px[k] = rn[0]; py[k] = rn[1]; pz[k] = rn[2];
+        ox[k] = en[0]; oy[k] = en[1]; oz[k] = en[2];
+        *de_out = de;
+    }
+    return acc;
+}
+
+/* the staged particles of the 27-cell stencil of cell (cx, cy, cz) */
+static int stage_stencil(const lco_grid *g, int cx, int cy, int cz, int *slots)
+{
+    int sc[27];
+    int ns = stencil_cells(g, cx, cy, cz, sc);
+    int S = 0;
+    for (int s = 0; s < ns; s++)
+        for (int q = g->cell_start[sc[s]]; q < g->cell_start[sc[s] + 1]; q++) slots[S++] = g->order[q];
+    return S;
+}
+
 int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n, double *px, double *py, double *pz,
               double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st, unsigned char *accept_bits,
               int *order_out)
@@ -776,70 +848,17 @@ int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n,
             for (int cy = by; cy < g.nc[1]; cy += 2)
                 for (int cx = bx; cx < g.nc[0]; cx += 2) {
                     int cell = (cz * g.nc[1] + cy) * g.nc[0] + cx;
-                    int sc[27];
-                    int ns = stencil_cells(&g, cx, cy, cz, sc);
-                    int S = 0;
-                    for (int s = 0; s < ns; s++)
-                        for (int q = g.cell_start[sc[s]]; q < g.cell_start[sc[s] + 1]; q++) slots[S++] = g.order[q];
+                    int S = stage_stencil(&g, cx, cy, cz, slots);
                     for (int a = g.cell_start[cell]; a < g.cell_start[cell + 1]; a++) {
                         int k = g.order[a];
                         if (order_out) order_out[st->attempted] = k;
                         st->attempted++;
-                        uint32_t rnd[4];
-                        philox_at(key, (uint32_t)k, sweep, TAG_MOVE, rnd);
-                        double ro[3] = {px[k], py[k], pz[k]}, eo[3] = {ox[k], oy[k], oz[k]};
-                        double rn[3];
-                        rn[0] = ro[0] + c->max_disp * (lco_u01(rnd[0]) - 0.5);
-                        rn[1] = ro[1] + c->max_disp * (lco_u01(rnd[1]) - 0.5);
-                        rn[2] = ro[2] + c->max_disp * (lco_u01(rnd[2]) - 0.5);
-                        lco_apply_pbc(&rn[0], &rn[1], &rn[2], box);
-                        double ddx, ddy, ddz;
-                        double rc2c = lco_distance_sq(rn[0], rn[1], rn[2], 0.5 * box[0], 0.5 * box[1], 0.5 * box[2], box,
-                                                      &ddx, &ddy, &ddz);
-                        if (!(rc2c > c->coll_R * c->coll_R)) {
-                            st->hardcore_rejected++;
-                            if (accept_bits) accept_bits[nb] = 2;
-                            nb++;
-                            continue;
-                        }
-                        double v[3];
-                        lco_sphere_point(key, (uint32_t)k, sweep, v);
-                        double en[3];
-                        en[0] = c->max_rot * v[0] + eo[0];
-                        en[1] = c->max_rot * v[1] + eo[1];
-                        en[2] = c->max_rot * v[2] + eo[2];
-                        double norm2 = en[0] * en[0] + en[1] * en[1] + en[2] * en[2];
-                        if (norm2 <= 1e-12) {
-                            en[0] = eo[0]; en[1] = eo[1]; en[2] = eo[2];
-                        } else {
-                            double nr = sqrt(norm2);
-                            en[0] /= nr; en[1] /= nr; en[2] /= nr;
-                        }
-                        double po[32], pn[32];
-                        memset(po, 0, sizeof(po));
-                        memset(pn, 0, sizeof(pn));
-                        for (int q = 0; q < S; q++) {
-                            int j = slots[q];
-                            if (j == k) continue;
-                            double rj[3] = {px[j], py[j], pz[j]}, ej[3] = {ox[j], oy[j], oz[j]};
-                            int in;
-                            double vo = lco_pair(c, ro, eo, rj, ej, box, &in);
-                            if (in) po[q & 31] += vo;
-                            double vn = lco_pair(c, rn, en, rj, ej, box, &in);
-                            if (in) pn[q & 31] += vn;
-                        }
-                        double Eo = butterfly32(po), En = butterfly32(pn);
-                        if (c->coll_on) {
-                            Eo = Eo + lco_colloid_rod(c, ro, eo, box);
-                            En = En + lco_colloid_rod(c, rn, en, box);
-                        }
-                        double de = En - Eo;
-                        int acc = (de <= 0.0) || (lco_log(lco_u01(rnd[3])) <= -c->beta * de);
-                        if (accept_bits) accept_bits[nb] = (unsigned char)acc;
+                        double de = 0.0;
+                        int r = attempt_move(c, key, sweep, k, slots, S, px, py, pz, ox, oy, oz, box, &de);
+                        if (accept_bits) accept_bits[nb] = (unsigned char)r;
                         nb++;
-                        if (acc) {
-                            px[k] = rn[0]; py[k] = rn[1]; pz[k] = rn[2];
-                            ox[k] = en[0]; oy[k] = en[1]; oz[k] = en[2];
+                        if (r == 2) st->hardcore_rejected++;
+                        if (r == 1) {
                             st->accepted++;
                             st->dE_sum += de;
                         }
@@ -847,6 +866,58 @@ int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n,
                 }
     }
     free(slots);
+    lco_grid_free(&g);
+    return 0;
+}
+
+/* lco_sweep with the active cells of each colour shared among threads
+ * (OpenMP, when this file is built with it): same-colour cells never interact,
+ * so the final state equals lco_sweep's bit for bit; dE_sum is summed in
+ * another order.  The CPU baseline's port of the checkerboard. */
+int lco_sweep_parallel(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n, double *px, double *py,
+                       double *pz, double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st)
+{
+    int nc[3];
+    for (int k = 0; k < 3; k++) lco_grid_dims(box[k], c->wmin, &nc[k]);
+    double shift[3];
+    lco_sweep_shift(key, sweep, nc, box, shift);
+    lco_grid g;
+    lco_grid_build(&g, n, px, py, pz, box, c->wmin, shift);
+    int perm[8];
+    lco_colour_order(key, sweep, perm);
+    long att = 0, acc = 0, hard = 0;
+    double dsum = 0.0;
+    for (int ci = 0; ci < 8; ci++) {
+        int col = perm[ci];
+        int bx = col & 1, by = (col >> 1) & 1, bz = (col >> 2) & 1;
+        int hx = (g.nc[0] - bx + 1) / 2, hy = (g.nc[1] - by + 1) / 2, hz = (g.nc[2] - bz + 1) / 2;
+        long ncell = (long)hx * hy * hz;
+#pragma omp parallel reduction(+ : att, acc, hard, dsum)
+        {
+            int *slots = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(dynamic, 4)
+            for (long e = 0; e < ncell; e++) {
+                int cx = bx + 2 * (int)(e % hx), cy = by + 2 * (int)((e / hx) % hy), cz = bz + 2 * (int)(e / ((long)hx * hy));
+                int cell = (cz * g.nc[1] + cy) * g.nc[0] + cx;
+                int S = stage_stencil(&g, cx, cy, cz, slots);
+                for (int a = g.cell_start[cell]; a < g.cell_start[cell + 1]; a++) {
+                    double de = 0.0;
+                    int r = attempt_move(c, key, sweep, g.order[a], slots, S, px, py, pz, ox, oy, oz, box, &de);
+                    att++;
+                    if (r == 2) hard++;
+                    if (r == 1) {
+                        acc++;
+                        dsum += de;
+                    }
+                }
+            }
+            free(slots);
+        }
+    }
+    st->attempted = att;
+    st->accepted = acc;
+    st->hardcore_rejected = hard;
+    st->dE_sum = dsum;
     lco_grid_free(&g);
     return 0;
 }

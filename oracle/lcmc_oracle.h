@@ -151,6 +151,12 @@ int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n,
               double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st, unsigned char *accept_bits,
               int *order_out);
 
+/* lco_sweep with each colour's active cells shared among OpenMP threads (in
+ * the -fopenmp build, oracle/_build/liblcmc_oracle_omp.so): the same final
+ * state; the checkerboard port timed as a CPU baseline. */
+int lco_sweep_parallel(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n, double *px, double *py,
+                       double *pz, double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st);
+
 /* Total energy over the cell stencil (cutoff rc, minimum image), FP64. */
 double lco_total_energy_cells(const lco_consts *c, int n, const double *px, const double *py, const double *pz,
                               const double *ox, const double *oy, const double *oz, const double box[3]);

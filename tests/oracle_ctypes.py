@@ -165,6 +165,33 @@ def sweep(c, k, sweep_index, state, box, record=False):
     return st, bits, order
 
 
+_omp = None
+
+
+def omp_lib():
+    """The OpenMP build of the oracle (lco_sweep_parallel's threads)."""
+    global _omp
+    if _omp is None:
+        so = os.path.join(ORACLE_DIR, "_build", "liblcmc_oracle_omp.so")
+        if not os.path.exists(so):
+            subprocess.check_call(["make", "-s", "-C", ORACLE_DIR])
+        L = C.CDLL(so)
+        L.lco_consts_from_params.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(Consts)]
+        L.lco_key.argtypes = [C.c_uint64, C.c_int, U32P]
+        L.lco_sweep_parallel.argtypes = [C.POINTER(Consts), U32P, C.c_uint64, C.c_int, DP, DP, DP, DP, DP, DP, DP,
+                                         C.POINTER(SweepStats)]
+        _omp = L
+    return _omp
+
+
+def sweep_parallel(c, k, sweep_index, state, box):
+    """lco_sweep_parallel (OpenMP over each colour's cells) on `state`, in place."""
+    st = SweepStats()
+    omp_lib().lco_sweep_parallel(C.byref(c), k, sweep_index, len(state[0]), *[ptr(x) for x in state], ptr(box),
+                                 C.byref(st))
+    return st
+
+
 def total_energy(c, state, box, allpairs=False):
     n = len(state[0])
     f = lib().lco_tot_ene if allpairs else lib().lco_total_energy_cells
