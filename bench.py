@@ -250,9 +250,10 @@ def dilute_start(n, rho0, R, seed):
 
 
 def npt_params(lcmc, n, T, P, R, seed, dlnv, cap=64):
-    """cap: active-cell capacity of the FP32 kernel (64, the large class, is what
-    the library picks for NPT systems by itself; 48 selects the small class,
-    enough at the density P* = 2 compresses these systems to)."""
+    """cap: active-cell capacity of the FP32 kernel (64: the large class, room
+    for the training replicas' compression to P* = 4; the library's own NPT
+    default is 56; 48, the small class, is enough at the density P* = 2
+    compresses these systems to)."""
     return lcmc.default_params(num_particles=n, system_density=0.06, system_temperature=T, system_pressure=P,
                                mc_ensemble_type=2, npt_max_dlnV=dlnv, colloid_wall_option=1, colloid_radius=R,
                                rng_seed=seed, precision_mode=1, cell_capacity=cap, **GB_NPT)
@@ -303,18 +304,18 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
     # the N = 262,144 system: compress from a dilute start, settle at dlnV_max
     # 0.01, then every arm from that one state with one seed
     n = 262144
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05, 56)) as s:
         st, box = dilute_start(n, 0.06, 8.0, 12)
         s.upload(*st, box)
         s.sweep(1000)
         st4, box4 = s.download()
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 13, 0.01)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 13, 0.01, 56)) as s:
         s.upload(*st4, box4)
         s.sweep(1000)
         st4, box4 = s.download()
     arms = {}
     for name in ("plain", "learned", "fp32_screen"):
-        with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01)) as s:
+        with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01, 56)) as s:
             s.upload(*st4, box4)
             if name == "learned":
                 s.set_surrogate(sur)

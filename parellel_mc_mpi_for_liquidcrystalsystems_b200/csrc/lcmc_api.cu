@@ -523,19 +523,18 @@ static void choose_kernels(lcmc_ctx *c)
         if (kern == 1) {
             c->any_fast = true;
             if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
-            // active-cell capacity: the caller's cell_capacity when given; else for
-            // NVT the mean occupancy + 12 + 50% (a dense liquid's cell counts
-            // fluctuate far less than that; overflow is flagged), and for NPT,
-            // whose box may compress far below its creation volume, the large class
+            // active-cell capacity: the caller's cell_capacity when given; else the
+            // mean occupancy + 12 + 50% (a dense liquid's cell counts fluctuate far
+            // less than that; overflow is flagged), and for NPT, whose box may
+            // compress far below its creation volume, at least the middle class
             int want;
             if (p.cell_capacity > 0) {
                 want = p.cell_capacity;
-            } else if (rp.ensemble == 2) {
-                want = fast_variant(fast_variant_count() - 1).amax;
             } else {
                 const double wcell = rp.L[0] / (double)nc;
                 const double mean = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]) * wcell * wcell * wcell;
                 want = (int)(1.5 * mean + 12.0);
+                if (rp.ensemble == 2) want = std::max(want, fast_variant(1).amax);
             }
             if (want > need_amax) need_amax = want;
         } else {
@@ -545,7 +544,10 @@ static void choose_kernels(lcmc_ctx *c)
         spec21 = spec21 && p.gb_mu_exponent == 2.0 && p.gb_nu_exponent == 1.0 && p.gb_sigma_sidetoside == 1.0;
     }
     c->need_amax = need_amax;
-    c->fast_variant = 2 * (need_amax > fast_variant(0).amax ? 1 : 0) + (spec21 ? 1 : 0);
+    int cls = fast_variant_count() - 1; // the smallest class that holds need_amax (else the largest)
+    for (int v = fast_variant_count() - 1; v >= 0; v--)
+        if (fast_variant(v).amax >= need_amax) cls = v;
+    c->fast_variant = 2 * cls + (spec21 ? 1 : 0);
 }
 
 static int upload_replica_table(lcmc_ctx *c)

@@ -106,10 +106,11 @@ __device__ __forceinline__ void cell_failed(const DevView &v, int r, int cell, i
     v.cell_cands[cell] = 0ull;
 }
 
-// resident CTAs per SM the register budget is sized for: the small capacity
-// class (36.9 KB of shared memory) fits six per SM at 80 registers, the large
-// class is limited to three by its shared memory
-template <int AMAX> struct FastMinBlocks { static constexpr int value = AMAX <= 48 ? 6 : 3; };
+// resident CTAs per SM the register budget is sized for: the 48-particle
+// class (36.9 KB of shared memory) fits six per SM at 80 registers, the
+// 56-particle class (44.5 KB) five at 102, the 64-particle class is limited to
+// three by its shared memory
+template <int AMAX> struct FastMinBlocks { static constexpr int value = AMAX <= 48 ? 6 : (AMAX <= 56 ? 5 : 3); };
 
 template <int NT, int AMAX, int SEG, int LW, bool SPEC21>
 __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(DevView v, int ci)
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
 namespace lcmc {
 
 // (threads, active capacity, staged candidates per warp segment, per-warp list capacity)
-static const FastVariant kVariants[] = {{128, 48, 176, 160}, {128, 64, 288, 384}};
+static const FastVariant kVariants[] = {{128, 48, 176, 160}, {128, 56, 192, 192}, {128, 64, 288, 384}};
 
 int fast_variant_count() { return (int)(sizeof(kVariants) / sizeof(kVariants[0])); }
 FastVariant fast_variant(int i) { return kVariants[i]; }
@@ -580,7 +581,9 @@ void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, in
     switch (variant) {
     case 0: launch_v<128, 48, 176, 160, false>(v, s, ci, grid); break;
     case 1: launch_v<128, 48, 176, 160, true>(v, s, ci, grid); break;
-    case 2: launch_v<128, 64, 288, 384, false>(v, s, ci, grid); break;
+    case 2: launch_v<128, 56, 192, 192, false>(v, s, ci, grid); break;
+    case 3: launch_v<128, 56, 192, 192, true>(v, s, ci, grid); break;
+    case 4: launch_v<128, 64, 288, 384, false>(v, s, ci, grid); break;
     default: launch_v<128, 64, 288, 384, true>(v, s, ci, grid); break;
     }
 }
@@ -592,7 +595,9 @@ int fast_blocks_per_sm(int variant)
     switch (variant) {
     case 0: return occupancy_v<128, 48, 176, 160, false>();
     case 1: return occupancy_v<128, 48, 176, 160, true>();
-    case 2: return occupancy_v<128, 64, 288, 384, false>();
+    case 2: return occupancy_v<128, 56, 192, 192, false>();
+    case 3: return occupancy_v<128, 56, 192, 192, true>();
+    case 4: return occupancy_v<128, 64, 288, 384, false>();
     default: return occupancy_v<128, 64, 288, 384, true>();
     }
 }

@@ -166,8 +166,8 @@ def test_adaptive_step_follows_the_reference_rule():
 
 
 def test_autotune_keeps_the_chain(tmp_path):
-    """lcmc_autotune times both phase-kernel capacity classes (11,000 rods, 8
-    cells per axis, ~22 per cell) and restores everything after each trial: the
+    """lcmc_autotune times the three phase-kernel capacity classes (11,000 rods,
+    8 cells per axis, ~22 per cell) and restores everything after each trial: the
     chain continues bit for bit as an untuned run's.  A second context with the
     same workload takes the choice from the cache file without timing."""
     p = lcmc.default_params(num_particles=11000, system_density=0.30, rng_seed=17, precision_mode=1, **COMMON)
@@ -177,8 +177,8 @@ def test_autotune_keeps_the_chain(tmp_path):
         s.sweep(3)
         before, _ = s.download()
         t = s.autotune(2, cache)
-        assert t["trials"] == 2 and not t["from_cache"] and t["ms_per_sweep"] > 0.0
-        assert t["capacity"] in (48, 64)
+        assert t["trials"] == 3 and not t["from_cache"] and t["ms_per_sweep"] > 0.0
+        assert t["capacity"] in (48, 56, 64)
         after, _ = s.download()
         for u, v in zip(before, after):
             assert np.array_equal(bits(u), bits(v))
@@ -204,7 +204,8 @@ def test_autotune_keeps_the_chain(tmp_path):
 
 def test_autotune_npt_volume_kernels():
     """For an NPT system with >= 4 cells per axis both kernels for the volume
-    move's energies are timed; state and statistics are untouched."""
+    move's energies are timed with each capacity class an NPT system may use
+    (56 and 64 particles); state and statistics are untouched."""
     p = lcmc.default_params(num_particles=11000, system_density=0.30, rng_seed=23, precision_mode=1,
                             mc_ensemble_type=2, system_pressure=2.0, system_temperature=1.2, npt_max_dlnV=0.01,
                             **COMMON)
@@ -214,7 +215,7 @@ def test_autotune_npt_volume_kernels():
         before, box0 = s.download()
         st0 = s.stats()
         t = s.autotune(1)
-        assert t["trials"] == 2 and t["capacity"] == 64
+        assert t["trials"] == 4 and t["capacity"] in (56, 64)
         after, box1 = s.download()
         for u, v in zip(before, after):
             assert np.array_equal(bits(u), bits(v))
