@@ -524,16 +524,29 @@ static void choose_kernels(lcmc_ctx *c)
             c->any_fast = true;
             if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
             // active-cell capacity: the caller's cell_capacity when given; else the
-            // mean occupancy + 12 + 50% (a dense liquid's cell counts fluctuate far
-            // less than that; overflow is flagged), and for NPT, whose box may
-            // compress far below its creation volume, at least the middle class
+            // mean occupancy m plus six standard deviations of the cell count plus
+            // 6, with the variance m S: S = 1 (Poisson) for a gas (rho* <= 0.15),
+            // 0.3 for a dense liquid (rho* >= 0.25, whose counts fluctuate far
+            // less), linear between, and at least what the lattice start puts in
+            // its fullest cell; overflow is flagged.  NPT systems, whose box may
+            // compress far below its creation volume, take at least the middle
+            // class.
             int want;
             if (p.cell_capacity > 0) {
                 want = p.cell_capacity;
             } else {
+                const double rho = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]);
                 const double wcell = rp.L[0] / (double)nc;
-                const double mean = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]) * wcell * wcell * wcell;
-                want = (int)(1.5 * mean + 12.0);
+                const double mean = rho * wcell * wcell * wcell;
+                const double S = rho >= 0.25 ? 0.3 : (rho <= 0.15 ? 1.0 : 1.0 - 0.7 * (rho - 0.15) / 0.10);
+                want = (int)std::ceil(mean + 6.0 * std::sqrt(mean * S) + 6.0);
+                // the lattice start: sites a = L / n_s apart, floor(w / a) + 1 per
+                // axis in the fullest cell
+                const double V = rp.L[0] * rp.L[1] * rp.L[2];
+                const double vcol = (4.0 / 3.0) * 3.1415926535898 * std::pow(p.colloid_radius, 3);
+                const int ns = (int)std::ceil(std::cbrt(p.num_particles / std::max(1e-3, 1.0 - vcol / V)) - 1e-9);
+                const int per_axis = (int)std::floor(wcell * ns / rp.L[0]) + 1;
+                want = std::max(want, per_axis * per_axis * per_axis);
                 if (rp.ensemble == 2) want = std::max(want, fast_variant(1).amax);
             }
             if (want > need_amax) need_amax = want;
