@@ -269,6 +269,15 @@ int lcmc_get_params(lcmc_ctx *ctx, int replica, lcmc_params *out);
  * draws from counters (seed, particle, s); set it to resume a run. */
 int lcmc_set_sweep_counter(lcmc_ctx *ctx, int replica, int64_t sweep);
 
+/* Active-cell capacity the FP32 kernel takes for a system created with *p (no
+ * counterpart in the reference, whose cells are unbounded host arrays): the
+ * caller's cell_capacity when given; else, from the creation density, the
+ * mean occupancy of a cell m plus six standard deviations of its count (variance
+ * m for a gas, rho* <= 0.15, and 0.3 m for a dense liquid, rho* >= 0.25) plus 6,
+ * at least what the lattice start puts in its fullest cell, and at least 56
+ * for NPT.  class_capacity: the kernel class used (48, 56 or 64).  Host only. */
+int lcmc_cell_capacity(const lcmc_params *p, int *capacity, int *class_capacity);
+
 /* Autotuner (no counterpart in the reference): times `sweeps` sweeps (after
  * one warm-up sweep) of every candidate configuration -- each FP32 phase-kernel
  * capacity class the capacity rule allows (the per-block tile of the active

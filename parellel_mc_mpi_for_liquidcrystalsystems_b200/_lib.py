@@ -106,6 +106,7 @@ EXPORTS = {
     "lcmc_get_step": ([C.c_void_p, C.c_int, DP, DP], C.c_int),
     "lcmc_set_sweep_counter": ([C.c_void_p, C.c_int, C.c_int64], C.c_int),
     "lcmc_autotune": ([C.c_void_p, C.c_int, C.c_char_p, C.POINTER(Tuning)], C.c_int),
+    "lcmc_cell_capacity": ([C.POINTER(Params), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "lcmc_write_fort1": ([C.c_char_p, C.c_int, DP, DP, DP, DP, DP, DP, DP, C.c_double], C.c_int),
     "lcmc_read_fort1": ([C.c_char_p, C.c_int, DP, DP, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_int)], C.c_int),
     "lcmc_write_trajectory": ([C.c_char_p, C.c_int, C.c_int, DP, DP, DP, DP, DP, DP, DP], C.c_int),

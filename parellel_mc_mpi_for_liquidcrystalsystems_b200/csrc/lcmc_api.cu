@@ -507,6 +507,51 @@ static void invalidate_graphs(lcmc_ctx *c)
         }
 }
 
+// Active-cell capacity the FP32 kernel needs for a system in a cubic box of
+// side L: the caller's cell_capacity when given; else the mean occupancy m
+// plus six standard deviations of a cell's count plus 6, with the variance m S:
+// S = 1 (Poisson) for a gas (rho* <= 0.15), 0.3 for a dense liquid (rho* >= 0.25,
+// whose counts fluctuate far less), linear between; and at least what the
+// lattice start puts in its fullest cell.  NPT systems, whose box may compress
+// far below its creation volume, take at least the middle class.  A cell above
+// the capacity is flagged after the sweep.
+static int capacity_rule(const lcmc_params &p, double L, double wmin, bool npt)
+{
+    if (p.cell_capacity > 0) return p.cell_capacity;
+    const int nc = grid_dim_host(L, wmin);
+    const double V = L * L * L;
+    const double rho = p.num_particles / V;
+    const double wcell = L / (double)nc;
+    const double mean = rho * wcell * wcell * wcell;
+    const double S = rho >= 0.25 ? 0.3 : (rho <= 0.15 ? 1.0 : 1.0 - 0.7 * (rho - 0.15) / 0.10);
+    int want = (int)std::ceil(mean + 6.0 * std::sqrt(mean * S) + 6.0);
+    // the lattice start: sites a = L / n_s apart, floor(w / a) + 1 per axis in the fullest cell
+    const double vcol = (4.0 / 3.0) * 3.1415926535898 * std::pow(p.colloid_radius, 3);
+    const int ns = (int)std::ceil(std::cbrt(p.num_particles / std::max(1e-3, 1.0 - vcol / V)) - 1e-9);
+    const int per_axis = (int)std::floor(wcell * ns / L) + 1;
+    want = std::max(want, per_axis * per_axis * per_axis);
+    if (npt) want = std::max(want, fast_variant(1).amax);
+    return want;
+}
+
+// the smallest capacity class that holds `want` (else the largest)
+static int capacity_class(int want)
+{
+    int cls = fast_variant_count() - 1;
+    for (int v = fast_variant_count() - 1; v >= 0; v--)
+        if (fast_variant(v).amax >= want) cls = v;
+    return cls;
+}
+
+extern "C" int lcmc_cell_capacity(const lcmc_params *p, int *capacity, int *class_capacity)
+{
+    if (!p || !capacity || !class_capacity || p->num_particles <= 0 || !(p->system_density > 0.0)) return LCMC_EINVAL;
+    const double L = box_length(*p);
+    *capacity = capacity_rule(*p, L, min_cell_width(*p), p->mc_ensemble_type == LCMC_NPT);
+    *class_capacity = fast_variant(capacity_class(*capacity)).amax;
+    return LCMC_OK;
+}
+
 // Kernel selection: FP32 kernel for precision_mode fp32 (boxes with >= 4
 // cells per axis; smaller boxes run the FP64 kernel), FP64 kernel otherwise.
 static void choose_kernels(lcmc_ctx *c)
@@ -523,32 +568,7 @@ static void choose_kernels(lcmc_ctx *c)
         if (kern == 1) {
             c->any_fast = true;
             if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
-            // active-cell capacity: the caller's cell_capacity when given; else the
-            // mean occupancy m plus six standard deviations of the cell count plus
-            // 6, with the variance m S: S = 1 (Poisson) for a gas (rho* <= 0.15),
-            // 0.3 for a dense liquid (rho* >= 0.25, whose counts fluctuate far
-            // less), linear between, and at least what the lattice start puts in
-            // its fullest cell; overflow is flagged.  NPT systems, whose box may
-            // compress far below its creation volume, take at least the middle
-            // class.
-            int want;
-            if (p.cell_capacity > 0) {
-                want = p.cell_capacity;
-            } else {
-                const double rho = p.num_particles / (rp.L[0] * rp.L[1] * rp.L[2]);
-                const double wcell = rp.L[0] / (double)nc;
-                const double mean = rho * wcell * wcell * wcell;
-                const double S = rho >= 0.25 ? 0.3 : (rho <= 0.15 ? 1.0 : 1.0 - 0.7 * (rho - 0.15) / 0.10);
-                want = (int)std::ceil(mean + 6.0 * std::sqrt(mean * S) + 6.0);
-                // the lattice start: sites a = L / n_s apart, floor(w / a) + 1 per
-                // axis in the fullest cell
-                const double V = rp.L[0] * rp.L[1] * rp.L[2];
-                const double vcol = (4.0 / 3.0) * 3.1415926535898 * std::pow(p.colloid_radius, 3);
-                const int ns = (int)std::ceil(std::cbrt(p.num_particles / std::max(1e-3, 1.0 - vcol / V)) - 1e-9);
-                const int per_axis = (int)std::floor(wcell * ns / rp.L[0]) + 1;
-                want = std::max(want, per_axis * per_axis * per_axis);
-                if (rp.ensemble == 2) want = std::max(want, fast_variant(1).amax);
-            }
+            const int want = capacity_rule(p, rp.L[0], rp.wmin, rp.ensemble == 2);
             if (want > need_amax) need_amax = want;
         } else {
             c->any_exact = true;
@@ -557,10 +577,7 @@ static void choose_kernels(lcmc_ctx *c)
         spec21 = spec21 && p.gb_mu_exponent == 2.0 && p.gb_nu_exponent == 1.0 && p.gb_sigma_sidetoside == 1.0;
     }
     c->need_amax = need_amax;
-    int cls = fast_variant_count() - 1; // the smallest class that holds need_amax (else the largest)
-    for (int v = fast_variant_count() - 1; v >= 0; v--)
-        if (fast_variant(v).amax >= need_amax) cls = v;
-    c->fast_variant = 2 * cls + (spec21 ? 1 : 0);
+    c->fast_variant = 2 * capacity_class(need_amax) + (spec21 ? 1 : 0);
 }
 
 static int upload_replica_table(lcmc_ctx *c)

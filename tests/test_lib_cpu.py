@@ -107,3 +107,23 @@ def test_no_gpu_is_a_loud_error():
     with pytest.raises(lcmc.LcmcError) as e:
         lcmc.GBSystem(p)
     assert e.value.code == _lib.ENODEV
+
+
+@pytest.mark.parametrize("kw,lo,cls", [
+    # the NVT bench system: ~22.5 rods per 4.13-wide cell of a dense liquid
+    (dict(num_particles=1048576, system_density=0.32, init_orientation_cone_deg=20.0), 40, 48),
+    # a gas (rho* = 0.1) in 6.5-wide cells: Poisson counts around 27
+    (dict(num_particles=1728, system_density=0.1, colloid_wall_option=1, colloid_radius=2.0, max_displacement=0.5),
+     57, 64),
+    # 4 cells per axis of 4.7: the lattice start puts 4 x 4 x 4 sites in the fullest cell
+    (dict(num_particles=2000, system_density=0.30, colloid_wall_option=1, colloid_radius=3.0), 64, 64),
+    # NPT: at least the middle class; explicit capacity wins
+    (dict(num_particles=11000, system_density=0.30, mc_ensemble_type=2), 56, 56),
+    (dict(num_particles=11000, system_density=0.30, mc_ensemble_type=2, cell_capacity=48), 48, 48),
+])
+def test_cell_capacity_rule(kw, lo, cls):
+    import ctypes as C
+    p = lcmc.default_params(**kw)
+    cap, klass = C.c_int(), C.c_int()
+    assert _lib.lib().lcmc_cell_capacity(C.byref(p), C.byref(cap), C.byref(klass)) == 0
+    assert cap.value >= lo and klass.value == cls, (cap.value, klass.value)
