@@ -515,21 +515,38 @@ static void invalidate_graphs(lcmc_ctx *c)
 // lattice start puts in its fullest cell.  NPT systems, whose box may compress
 // far below its creation volume, take at least the middle class.  A cell above
 // the capacity is flagged after the sweep.
+// particles the lattice start puts in its fullest cell: sites a = L / n_s
+// apart, floor(w / a) + 1 per axis
+static int lattice_fullest_cell(const lcmc_params &p, double L, double wmin)
+{
+    const int nc = grid_dim_host(L, wmin);
+    const double V = L * L * L;
+    const double vcol = (4.0 / 3.0) * 3.1415926535898 * std::pow(p.colloid_radius, 3);
+    const int ns = (int)std::ceil(std::cbrt(p.num_particles / std::max(1e-3, 1.0 - vcol / V)) - 1e-9);
+    const int per_axis = (int)std::floor((L / (double)nc) * ns / L) + 1;
+    return per_axis * per_axis * per_axis;
+}
+
+// mean occupancy of a cell and the standard deviation of its count (variance
+// m S: S = 1, Poisson, for a gas, rho* <= 0.15; 0.3 for a dense liquid,
+// rho* >= 0.25, whose counts fluctuate far less; linear between)
+static void cell_count_stats(const lcmc_params &p, double L, double wmin, double *mean, double *sd)
+{
+    const int nc = grid_dim_host(L, wmin);
+    const double rho = p.num_particles / (L * L * L);
+    const double wcell = L / (double)nc;
+    const double S = rho >= 0.25 ? 0.3 : (rho <= 0.15 ? 1.0 : 1.0 - 0.7 * (rho - 0.15) / 0.10);
+    *mean = rho * wcell * wcell * wcell;
+    *sd = std::sqrt(*mean * S);
+}
+
 static int capacity_rule(const lcmc_params &p, double L, double wmin, bool npt)
 {
     if (p.cell_capacity > 0) return p.cell_capacity;
-    const int nc = grid_dim_host(L, wmin);
-    const double V = L * L * L;
-    const double rho = p.num_particles / V;
-    const double wcell = L / (double)nc;
-    const double mean = rho * wcell * wcell * wcell;
-    const double S = rho >= 0.25 ? 0.3 : (rho <= 0.15 ? 1.0 : 1.0 - 0.7 * (rho - 0.15) / 0.10);
-    int want = (int)std::ceil(mean + 6.0 * std::sqrt(mean * S) + 6.0);
-    // the lattice start: sites a = L / n_s apart, floor(w / a) + 1 per axis in the fullest cell
-    const double vcol = (4.0 / 3.0) * 3.1415926535898 * std::pow(p.colloid_radius, 3);
-    const int ns = (int)std::ceil(std::cbrt(p.num_particles / std::max(1e-3, 1.0 - vcol / V)) - 1e-9);
-    const int per_axis = (int)std::floor(wcell * ns / L) + 1;
-    want = std::max(want, per_axis * per_axis * per_axis);
+    double mean, sd;
+    cell_count_stats(p, L, wmin, &mean, &sd);
+    int want = (int)std::ceil(mean + 6.0 * sd + 6.0);
+    want = std::max(want, lattice_fullest_cell(p, L, wmin));
     if (npt) want = std::max(want, fast_variant(1).amax);
     return want;
 }
@@ -563,6 +580,13 @@ static void choose_kernels(lcmc_ctx *c)
         Replica &rp = c->rep[r];
         const lcmc_params &p = c->params[r];
         int kern = c->kernel_override >= 0 ? c->kernel_override : (p.precision_mode == LCMC_PREC_FP32 ? 1 : 0);
+        // an FP32 system whose cells the capacity rule puts above the largest
+        // class (wide cells of a small box, or a gas) runs on the FP64 kernel,
+        // which has no cell capacity, unless the caller chose the kernel or set
+        // cell_capacity
+        if (kern == 1 && c->kernel_override < 0 && p.cell_capacity <= 0 &&
+            capacity_rule(p, rp.L[0], rp.wmin, rp.ensemble == 2) > fast_variant(fast_variant_count() - 1).amax)
+            kern = 0;
         rp.kernel = kern;
         int nc = grid_dim_host(rp.L[0], rp.wmin);
         if (kern == 1) {
@@ -748,14 +772,12 @@ extern "C" int lcmc_set_kernel(lcmc_ctx *ctx, int kernel)
 {
     if (!ctx || kernel < -1 || kernel > 1) return LCMC_EINVAL;
     ctx->kernel_override = kernel;
-    // the device table keeps the dynamic fields; only `kernel` changes
-    for (int r = 0; r < ctx->R; r++) {
-        int kern = kernel >= 0 ? kernel : (ctx->params[r].precision_mode == LCMC_PREC_FP32 ? 1 : 0);
-        CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * r + offsetof(Replica, kernel), &kern,
-                                      sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    }
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     choose_kernels(ctx);
+    // the device table keeps the dynamic fields; only `kernel` changes
+    for (int r = 0; r < ctx->R; r++)
+        CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * r + offsetof(Replica, kernel),
+                                      &ctx->rep[r].kernel, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->grid_fast = fast_blocks_per_sm(ctx->fast_variant) * ctx->sms;
     invalidate_graphs(ctx);
     return LCMC_OK;

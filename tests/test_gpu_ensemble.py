@@ -29,7 +29,8 @@ def test_ensemble_matches_reference_chain(golden, precision):
     common = dict(num_particles=n, system_density=float(g["rho"]), system_temperature=float(g["T"]),
                   colloid_wall_option=1, colloid_radius=float(g["colloid_R"]), gb_kappa=3.0, gb_kappa_prime=5.0,
                   gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
-                  max_displacement=float(g["dmax"]), max_rotation=float(g["rot"]), precision_mode=precision)
+                  max_displacement=float(g["dmax"]), max_rotation=float(g["rot"]), precision_mode=precision,
+                  cell_capacity=64)  # the gas's ~27 rods per cell: the largest FP32 class, chosen explicitly
     start, box = lcmc.lattice(lcmc.default_params(rng_seed=int(g["seed"]), **common))
     ps = [lcmc.default_params(rng_seed=9000 + 17 * r, **common) for r in range(REPLICAS)]
     with lcmc.GBSystem(ps) as s:
