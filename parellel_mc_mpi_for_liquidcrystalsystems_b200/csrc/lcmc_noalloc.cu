@@ -12,6 +12,7 @@
 // Compiled without FMA contraction, like the FP64 sweep kernel.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <mutex>
 
@@ -240,32 +241,48 @@ int total_energy_noalloc(const GBConsts &k, int n, const double *px, const doubl
     a.k = k;
     a.n = n;
     a.ncell = 1;
-    for (int d = 0; d < 3; d++) {
-        a.L[d] = box[d];
-        int m = (int)(box[d] / k.rc);
-        a.nc[d] = m < 1 ? 1 : m;
-        a.w[d] = box[d] / (double)a.nc[d];
-        a.ncell *= a.nc[d];
+    if (n > NA_MAX_N) {
+        snprintf(msg, len, "n = %d above the allocation-free limit of %d particles", n, NA_MAX_N);
+        return LCMC_EINVAL;
     }
+    // every size check runs before the first launch; the cell count per axis
+    // and their product are formed in 64 bits from finite boxes only, so a
+    // huge or non-finite box cannot wrap into a small (or negative) count
+    for (int d = 0; d < 3; d++) {
+        if (!std::isfinite(box[d])) {
+            snprintf(msg, len, "box edge %d is not finite", d);
+            return LCMC_EINVAL;
+        }
+    }
+    if (!(box[0] >= 2.0 * k.rc && box[1] >= 2.0 * k.rc && box[2] >= 2.0 * k.rc)) {
+        snprintf(msg, len, "box shorter than twice the cutoff");
+        return LCMC_EBOX;
+    }
+    long long ncell = 1;
+    for (int d = 0; d < 3; d++) {
+        const double m = std::floor(box[d] / k.rc);
+        if (!(m <= (double)NA_MAX_C)) {
+            snprintf(msg, len, "box edge %d gives more than %d cells per axis (allocation-free limit %d cells)", d,
+                     NA_MAX_C, NA_MAX_C);
+            return LCMC_EINVAL;
+        }
+        a.nc[d] = m < 1.0 ? 1 : (int)m;
+        a.L[d] = box[d];
+        a.w[d] = box[d] / (double)a.nc[d];
+        ncell *= (long long)a.nc[d];
+    }
+    if (ncell > (long long)NA_MAX_C) {
+        snprintf(msg, len, "%d x %d x %d cells above the allocation-free limit of %d", a.nc[0], a.nc[1], a.nc[2],
+                 NA_MAX_C);
+        return LCMC_EINVAL;
+    }
+    a.ncell = (int)ncell;
     a.px = px;
     a.py = py;
     a.pz = pz;
     a.ox = ox;
     a.oy = oy;
     a.oz = oz;
-    if (n > NA_MAX_N) {
-        snprintf(msg, len, "n = %d above the allocation-free limit of %d particles", n, NA_MAX_N);
-        return LCMC_EINVAL;
-    }
-    if (a.ncell > NA_MAX_C) {
-        snprintf(msg, len, "%d x %d x %d cells above the allocation-free limit of %d", a.nc[0], a.nc[1], a.nc[2],
-                 NA_MAX_C);
-        return LCMC_EINVAL;
-    }
-    if (!(box[0] >= 2.0 * k.rc && box[1] >= 2.0 * k.rc && box[2] >= 2.0 * k.rc)) {
-        snprintf(msg, len, "box shorter than twice the cutoff");
-        return LCMC_EBOX;
-    }
     NoAllocScratch *s = nullptr;
     int rc = noalloc_scratch(&s, msg, len);
     if (rc) return rc;

@@ -80,3 +80,45 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
                                                box.ctypes.data_as(_lib.DP), C.c_void_p(dummy.data_ptr()), None)
     assert rc == _lib.EINVAL
     assert "limit" in _lib.last_error()
+
+
+def _call_with_box(torch, n, box):
+    p = lcmc.default_params(num_particles=max(n, 1), system_density=0.3, **COMMON)
+    dummy = torch.zeros(16, dtype=torch.float64, device="cuda")
+    b = np.ascontiguousarray(box, dtype=np.float64)
+    return _lib.lib().lcmc_total_energy_noalloc(C.byref(p), n, *[C.c_void_p(dummy.data_ptr())] * 6,
+                                                 b.ctypes.data_as(_lib.DP), C.c_void_p(dummy.data_ptr()), None)
+
+
+def test_noalloc_rejects_cell_grids_beyond_its_limit_before_launching():
+    """Every size check runs on the host before the first launch, so these
+    calls return an error and enqueue nothing (the dummy device arrays are
+    never read)."""
+    torch = pytest.importorskip("torch")
+    # 33 x 33 x 33 cells = 35,937 > 32,768
+    assert _call_with_box(torch, 10, [33 * 4.0 + 1.0] * 3) == _lib.EINVAL
+    assert "limit" in _lib.last_error()
+    # 1300^3 cells: the product overflows a 32-bit int (2.197e9 wraps negative)
+    assert _call_with_box(torch, 10, [5200.0] * 3) == _lib.EINVAL
+    # one axis alone past the limit
+    assert _call_with_box(torch, 10, [4.0 * 40000, 8.0, 8.0]) == _lib.EINVAL
+    # non-finite edges
+    assert _call_with_box(torch, 10, [np.inf, 20.0, 20.0]) == _lib.EINVAL
+    assert _call_with_box(torch, 10, [np.nan, 20.0, 20.0]) == _lib.EINVAL
+    # shorter than twice the cutoff
+    assert _call_with_box(torch, 10, [7.9, 20.0, 20.0]) == _lib.EBOX
+    torch.cuda.synchronize()
+
+
+def test_noalloc_empty_configuration_has_zero_energy():
+    torch = pytest.importorskip("torch")
+    p = lcmc.default_params(num_particles=1, system_density=0.3, **COMMON)
+    out = torch.full((1,), 123.0, dtype=torch.float64, device="cuda")
+    dummy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    box = np.array([20.0, 20.0, 20.0])
+    for _ in range(2):
+        rc = _lib.lib().lcmc_total_energy_noalloc(C.byref(p), 0, *[C.c_void_p(dummy.data_ptr())] * 6,
+                                                   box.ctypes.data_as(_lib.DP), C.c_void_p(out.data_ptr()), None)
+        assert rc == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        assert float(out.item()) == 0.0
