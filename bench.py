@@ -3,9 +3,14 @@
 
 Workload (one system per GPU, weak scaling over GPUs): GB(kappa=3, kappa'=5,
 mu=2, nu=1), N = 1,048,576 ellipsoids, rho* = 0.32, T* = 0.8, cutoff 4.0,
-max displacement 0.1, max rotation 0.1, NVT, seeded simple-cubic lattice
-with orientations within 20 degrees of z; FP32 pair terms, FP64 state and
-sums.  A step is one checkerboard sweep (N trial moves).
+max displacement 0.1, max rotation 0.1, NVT, seeded lattice start with
+orientations within 20 degrees of z: a body-centred tetragonal lattice with
+layers 1.05 sigma_ee apart along z (no pair in the 1e9 overlap clamp; tilted
+neighbours overlap mildly and relax in a few sweeps); FP32 pair terms,
+FP64 state and sums.  A step is one checkerboard sweep (N trial moves).  The
+line's `jammed_start` sub-object times the same system from the simple-cubic
+lattice (spacing 1.46 for rods of length 3: pairs in the 1e9 overlap clamp
+and terms up to 1e36 beside it, attempted in FP64 by the hand-over kernel).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -40,19 +45,53 @@ UNIT = "moves/s"
 N_PART = 1048576
 WORKLOAD = {
     "workload": "Gay-Berne NVT sweep, N=1048576, rho*=0.32, T*=0.8, GB(3,5,2,1), rc=4.0, d=0.1, rot=0.1, "
-                "lattice start with orientations within 20 deg of z",
+                "lattice start (body-centred tetragonal, layers 1.05 sigma_ee apart along z) with orientations "
+                "within 20 deg of z",
     "n_particles": N_PART,
     "precision": "fp32 pair terms, fp64 state and sums",
 }
 
 
-def gb_params(lcmc, seed):
+def gb_params(lcmc, seed, lattice=1):
+    """lattice 1: body-centred tetragonal start (the headline); 0: the
+    reference's simple-cubic lattice (jammed at this density)."""
     return lcmc.default_params(
         mc_ensemble_type=1, num_particles=N_PART, system_density=0.32, system_temperature=0.8,
         gb_sigma_sidetoside=1.0, gb_epsilon0=1.0, gb_kappa=3.0, gb_kappa_prime=5.0, gb_mu_exponent=2.0,
         gb_nu_exponent=1.0, max_displacement=0.1, max_rotation=0.1, cutoff_radius=4.0, verlet_radius=4.8,
         colloid_wall_option=0, colloid_radius=0.0, init_orientation_cone_deg=20.0, precision_mode=1,
-        rng_seed=seed)
+        rng_seed=seed, init_lattice=lattice)
+
+
+def bct_lattice(n, rho, seed, cone_deg, kappa=3.0):
+    """The workload's start for the CPU arms (which load none of this
+    library): the library's body-centred tetragonal sites (layers
+    c = L / floor(L / (1.05 kappa)) apart along z, square sites a = L / n_a
+    apart, the smallest n_a holding n, surplus sites left empty evenly),
+    orientations uniform on the cap within cone_deg of z from numpy's
+    generator (same distribution, other draws)."""
+    import numpy as np
+    L = (n / rho) ** (1.0 / 3.0)
+    nz = max(1, int(np.floor(L / (1.05 * kappa))))
+    c = L / nz
+    na = 1
+    while 2 * na * na * nz < n:
+        na += 1
+    a = L / na
+    S = 2 * na * na * nz
+    s = np.arange(S)
+    keep = ((s + 1) * n) // S > (s * n) // S
+    s = s[keep]
+    b, q = s & 1, s >> 1
+    ix, iy, iz = q % na, (q // na) % na, q // (na * na)
+    x = (ix + 0.5 * b) * a
+    y = (iy + 0.5 * b) * a
+    z = (iz + 0.5 * b) * c
+    rng = np.random.default_rng(seed)
+    ct = 1.0 - rng.random(n) * (1.0 - np.cos(np.radians(cone_deg)))
+    st = np.sqrt(1.0 - ct * ct)
+    ph = 2.0 * np.pi * rng.random(n)
+    return [np.ascontiguousarray(v) for v in (x, y, z, st * np.cos(ph), st * np.sin(ph), ct)], np.array([L, L, L])
 
 
 # ---------------------------------------------------------------------------
@@ -149,7 +188,7 @@ def reference_cpu(n_part, seconds=12.0, threads=None):
         path = f.name
     ref.load_initial_conditions(path.encode())
     os.unlink(path)
-    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=n_part, rho=0.32, seed=1234, cone=20.0)
+    (px, py, pz, ox, oy, oz), box = bct_lattice(n_part, 0.32, 1234, 20.0)
     ref.refdrv_set_box(n_part, box.ctypes.data_as(DP))
     libc = C.CDLL("libc.so.6")
     libc.srand(1234)
@@ -413,8 +452,7 @@ def port_cpu(n_part, seconds=8.0, threads=None):
         oc.omp_lib()
     except OSError as e:
         return None, f"oracle OpenMP build not loadable: {e}"
-    *state, box = oc.init_lattice(n=n_part, rho=0.32, seed=1234, cone=20.0)
-    state = [np.ascontiguousarray(x) for x in state]
+    state, box = bct_lattice(n_part, 0.32, 1234, 20.0)
     p = oc.params(num_particles=n_part, system_density=0.32, system_temperature=0.8, max_displacement=0.1,
                   max_rotation=0.1, cutoff_radius=4.0, rng_seed=1234, init_orientation_cone_deg=20.0)
     consts = oc.Consts()
@@ -433,6 +471,60 @@ def port_cpu(n_part, seconds=8.0, threads=None):
             "sample": f"{done} sweep(s) of the oracle's FP64 checkerboard (cell lists, lco_sweep_parallel) at "
                       f"N={n_part} from the workload's lattice start in {dt:.1f} s, OpenMP threads={threads}",
             "seconds": dt}, None
+
+
+# ---------------------------------------------------------------------------
+# FP64 energy check of the running energy (EnergyCheck, MCnptColloid.c:1343-1362)
+# ---------------------------------------------------------------------------
+def energy_check_record(lcmc, s, sweeps):
+    """Run the library's FP64 energy check on system s (outside any timed
+    region) and describe it; ok = False when the running energy was outside
+    the check's tolerance."""
+    try:
+        s.energy_check()
+        ok = True
+    except lcmc.LcmcError:
+        ok = False
+    st = s.stats()
+    n = s.params[0].num_particles
+    return {"ok": ok, "running_energy_per_particle": (st["last_recompute"] + st["drift"]) / n,
+            "recomputed_energy_per_particle": st["last_recompute"] / n, "drift": st["drift"],
+            "tolerance": st["drift_bound"], "breaches": st["drift_breaches"],
+            "fp64_cells_per_sweep": st["fp64_cells"] / max(1, sweeps),
+            "overcap_cells": st["overcap_cells"]}
+
+
+def jammed_start(lcmc, torch, steps, warmup):
+    """The same system from the reference's simple-cubic lattice (spacing 1.46
+    for rods of length 3 within 20 deg of z): overlapping pairs in the 1e9
+    clamp and terms up to 1e36 beside it, attempted in FP64 by the hand-over
+    kernel.  Device time per sweep, L2 flushed between sweeps."""
+    s = lcmc.GBSystem(gb_params(lcmc, 4321, lattice=0))
+    s.get_initial_config()
+    e0 = s.stats()["energy"] / N_PART
+    ext = torch.cuda.ExternalStream(s.stream_handle())
+    s.sweep(max(3, warmup))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    st0 = s.stats()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        s.sweep(1)
+        b.record(ext)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    st1 = s.stats()
+    chk = energy_check_record(lcmc, s, max(3, warmup) + steps)
+    chk["fp64_cells_per_sweep_timed"] = (st1["fp64_cells"] - st0["fp64_cells"]) / steps
+    s.close()
+    return {"workload": "as the headline, from the simple-cubic lattice (spacing L/102 = 1.46)",
+            "start_energy_per_particle": e0, "steps": steps, "warmup": max(3, warmup),
+            "ms_per_step": statistics.mean(ms), "value": N_PART * steps / (sum(ms) * 1e-3), "unit": UNIT,
+            "acceptance": (st1["accepted"] - st0["accepted"]) / max(1, st1["attempted"] - st0["attempted"]),
+            "energy_check": chk}
 
 
 # ---------------------------------------------------------------------------
@@ -473,6 +565,8 @@ def main():
                     help="npt: time NPT sweeps of one compressed system (per-part device times) instead")
     ap.add_argument("--npt-n", type=int, default=262144)
     ap.add_argument("--npt-screen", action="store_true", help="npt workload with the FP32-pair volume screen")
+    ap.add_argument("--jammed-steps", type=int, default=5,
+                    help="timed sweeps of the simple-cubic (jammed) start sub-measurement (0 skips it)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -542,6 +636,7 @@ def main():
     if dist:
         dist.barrier()
     st1 = s.stats()
+    check = energy_check_record(lcmc, s, max(3, args.warmup) + args.steps)
     attempted = st1["attempted"] - st0["attempted"]
     value = job_rate(N_PART * args.steps, world, total_ms * 1e-3)
 
@@ -577,6 +672,9 @@ def main():
     st = s.stats()
     e_exact = s.tot_ene()  # FP64 recompute of the final state (outside the timed region)
     s.close()
+    jam = None
+    if args.jammed_steps > 0 and world == 1:
+        jam = jammed_start(lcmc, torch, args.jammed_steps, args.warmup)
 
     if rank != 0:
         if dist:
@@ -618,11 +716,14 @@ def main():
         "cpu_baseline": cpu if cpu else {"unavailable": why},
         "cpu_port": port if port else {"unavailable": port_why},
         "acceptance": (st["accepted"] / max(st["attempted"], 1)),
-        # the lattice start holds overlapping rods (pair terms up to ~1e36), so the
-        # running FP64 energy carries their rounding; the recompute is the state's energy
+        # FP64 energy check after the timed sweeps (running vs recomputed, tolerance)
+        "energy_check": check,
+        # after the e2e steps: running energy carried through the C ABI vs an FP64 recompute
         "energy_per_particle": e_exact / N_PART,
         "running_energy_per_particle": st["energy"] / N_PART,
     }
+    if jam:
+        line["jammed_start"] = jam
     if clocks:
         line["clocks"] = clocks
     if peaks:
@@ -632,6 +733,9 @@ def main():
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+    if not check["ok"]:
+        sys.stderr.write("bench: the running energy failed the FP64 energy check\n")
+        return 3
     return 0
 
 

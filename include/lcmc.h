@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define LCMC_ABI_VERSION 1
+#define LCMC_ABI_VERSION 2
 
 enum {
     LCMC_OK = 0,
@@ -45,7 +45,10 @@ enum {
     LCMC_EBOX = -8,      /* box too small for the cutoff (L < 2 rc) or inconsistent sizes */
     LCMC_ENODEV = -9,    /* no CUDA device */
     LCMC_EOVERLAP = -10, /* a particle centre inside the colloid (check_no_colloid_overlaps, MCnptColloid.c:1324-1340) */
-    LCMC_ETIMEOUT = -11  /* a bounded wait inside a tensor-core kernel gave up (the kernel returned cleanly) */
+    LCMC_ETIMEOUT = -11, /* a bounded wait inside a tensor-core kernel gave up (the kernel returned cleanly) */
+    LCMC_EDRIFT = -12    /* a periodic FP64 energy check found the running energy out of tolerance
+                            (EnergyCheck, MCnptColloid.c:1343-1362, only prints); the running energy
+                            was reset to the recomputed value and the chain is unchanged */
 };
 
 enum { LCMC_PREC_FP64 = 0, LCMC_PREC_FP32 = 1 };
@@ -84,13 +87,24 @@ typedef struct {
     int total_mc_sweeps;             /* sweeps of a run_simulation driver run; 0 = ceil(total_mc_cycles / num_particles) */
     int cell_capacity;               /* active-cell capacity of the FP32 kernel (<= 48: small class, six
                                         blocks per SM; <= 64: large class); 0 = automatic: NVT from the
-                                        creation density, NPT the large class */
+                                        creation density, NPT the large class.  A cell holding more
+                                        particles is attempted in FP64 (counted in overcap_cells) */
     double npt_max_dlnV;
     int volume_moves_per_sweep;      /* 0 or 1 */
     int precision_mode;              /* LCMC_PREC_FP64 / LCMC_PREC_FP32 */
     double init_orientation_cone_deg;/* 180 = uniform on the sphere */
     int n_read;                      /* out: number of reference keys found */
     int missing_mask;                /* out: bit i = reference key i missing */
+    /* added keys (continued) */
+    int energy_check_interval;       /* sweeps between periodic FP64 energy checks, 0 = off (the reference's
+                                        check_energy / EnergyCheck, MCnptColloid.c:946-955, 1343-1362) */
+    double energy_check_tolerance;   /* relative tolerance of the check against max(|E|, N 4 eps0) plus the
+                                        sum of |dE| accepted since the last check; 0 = automatic: 1e-6 for
+                                        the FP32 kernel, 1e-9 for the FP64 kernel */
+    int init_lattice;                /* lattice of initial_configuration_type 2: 0 = simple cubic (the
+                                        reference's), 1 = body-centred tetragonal with the long axis along z,
+                                        spacing 1.05 sigma_ee along z (a start for orientations near z
+                                        with no pair in the overlap clamp) */
 } lcmc_params;
 
 typedef struct {
@@ -109,15 +123,23 @@ typedef struct {
     int error_flags;             /* LCMC_F* bits seen by the kernels */
     int kernel;                  /* 0 = FP64 kernel, 1 = FP32 kernel */
     int64_t volume_stage1_rejected; /* volume moves the surrogate rejected (no exact energy computed) */
+    int64_t fp64_cells;          /* FP32-kernel cell attempts run in FP64: a pair term above 100 eps0 (an
+                                    overlap), or the cell above the kernel's capacity */
+    int64_t overcap_cells;       /* of which: above the cell, staged-candidate or list capacity */
+    int64_t energy_checks;       /* periodic FP64 energy checks run */
+    int64_t drift_breaches;      /* checks out of tolerance */
+    double drift_bound;          /* tolerance of the last check (absolute energy) */
+    double abs_dE_since_check;   /* sum of |dE| of accepted moves since the last check */
 } lcmc_stats;
 
 /* error_flags bits */
 enum {
-    LCMC_F_CELLCAP = 1,     /* cell above the active capacity: that cell made no moves */
-    LCMC_F_STENCILCAP = 2,  /* stencil above the candidate capacity: that cell made no moves */
-    LCMC_F_LISTCAP = 4,     /* neighbour-list capacity exceeded: that cell made no moves */
+    LCMC_F_CELLCAP = 1,     /* not set by this version: a cell above the FP32 kernel's capacity (active,    */
+    LCMC_F_STENCILCAP = 2,  /* staged-candidate or list) is attempted in FP64 and counted in overcap_cells; */
+    LCMC_F_LISTCAP = 4,     /* the bits stay reserved                                                       */
     LCMC_F_NONFINITE = 8,   /* NaN/Inf energy change */
-    LCMC_F_GRIDCAP = 16     /* box grew past the allocated cell grid (cells kept wider) */
+    LCMC_F_GRIDCAP = 16,    /* box grew past the allocated cell grid (cells kept wider) */
+    LCMC_F_DRIFT = 32       /* a periodic FP64 energy check was out of tolerance */
 };
 
 /* ---- parameters (host only) ---- */
@@ -179,6 +201,27 @@ int lcmc_last_outcomes(lcmc_ctx *ctx, int replica, unsigned char *out, int n);
 /* Override the kernel choice (for tests): -1 auto, LCMC_PREC_FP64, LCMC_PREC_FP32. */
 int lcmc_set_kernel(lcmc_ctx *ctx, int kernel);
 
+/* Error flags are sticky: lcmc_sweep keeps returning the error of a set flag
+ * until the caller clears them. */
+int lcmc_clear_error_flags(lcmc_ctx *ctx);
+
+/* FP64 energy check now (the reference's EnergyCheck, MCnptColloid.c:1343-1362,
+ * which prints the running and the recomputed energy): recomputes every
+ * replica's total energy in FP64, records drift = running - recomputed,
+ * resets the running energy to the recomputed value and returns LCMC_EDRIFT
+ * (setting LCMC_F_DRIFT) when |drift| exceeds the replica's tolerance (see
+ * energy_check_tolerance).  lcmc_sweep runs the same check after every
+ * energy_check_interval sweeps of a replica.  The chain is unchanged. */
+int lcmc_energy_check(lcmc_ctx *ctx);
+
+/* Per-particle record of the moves of each sweep (for tests that compare
+ * kernels decision by decision): on = 1 starts recording, 0 stops and frees.
+ * lcmc_get_move_records returns, by particle id, the energy change dE of the
+ * last sweep's attempt (0 for a colloid hard-core reject) and the log of its
+ * Metropolis draw ln u (accepted iff dE <= 0 or ln u <= -beta dE). */
+int lcmc_record_moves(lcmc_ctx *ctx, int on);
+int lcmc_get_move_records(lcmc_ctx *ctx, int replica, double *dE, double *log_u, int n);
+
 /* ---- measurement (no counterpart in the reference, which only times with clock()) ---- */
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
 int lcmc_get_stream(lcmc_ctx *ctx, void **stream);
@@ -186,7 +229,8 @@ int lcmc_get_stream(lcmc_ctx *ctx, void **stream);
 int lcmc_kernels_per_sweep(lcmc_ctx *ctx);
 /* Device time of the last sweep run by lcmc_sweep, part by part, from CUDA
  * event nodes inside the sweep graph: ms[0] rebin, ms[1] the colour-phase
- * kernels (all 8 phases), ms[2] volume move, ms[3] finalize. */
+ * kernels (all 8 phases), ms[2] the phases' statistics and the volume move,
+ * ms[3] the sweep counter (and history). */
 int lcmc_last_sweep_timing(lcmc_ctx *ctx, double ms[4]);
 
 /* Gay-Berne pair term of n given configurations on the GPU, in the FP32
@@ -218,6 +262,14 @@ int lcmc_mlp_set_params(lcmc_mlp *m, const float *params);
 /* C[M x N] = A[M x K] B[N x K]^T with A, B rounded to BF16, FP32 accumulate, on
  * the tensor cores (host arrays; K a multiple of 64).  For tests. */
 int lcmc_gemm_bf16(const float *A, const float *B, float *C, int M, int N, int K);
+/* Limit, in tries, of the tensor-core kernels' bounded mbarrier waits for
+ * launches made from now on (0 restores the default, 2^24).  A wait that runs
+ * out sets the kernel's error flag, waits (with the full bound) for the MMAs
+ * it issued, frees its TMEM and returns; the call then reports LCMC_ETIMEOUT.
+ * For tests of that path (a limit of 1 makes the first wait give up).  Sweep
+ * graphs captured earlier keep the limit they were captured with.  No
+ * counterpart in the reference. */
+int lcmc_set_wait_limit(unsigned int tries);
 
 /* Delayed-acceptance volume moves (Christen & Fox 2005) for the NPT replicas of
  * a context: stage 1 tests the surrogate's energy change

@@ -11,7 +11,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "liblcmc.so")
 
 OK = 0
-EINVAL, ENOFILE, EPARAM, ECUDA, ENOMEM, ECELLCAP, ENUMERIC, EBOX, ENODEV, EOVERLAP = range(-1, -11, -1)
+EINVAL, ENOFILE, EPARAM, ECUDA, ENOMEM, ECELLCAP, ENUMERIC, EBOX, ENODEV, EOVERLAP, ETIMEOUT, EDRIFT = range(-1, -13, -1)
+F_DRIFT = 32
 PREC_FP64, PREC_FP32 = 0, 1
 NVT, NPT = 1, 2
 
@@ -34,6 +35,7 @@ class Params(C.Structure):
         ("colloid_radius", D), ("rng_seed", C.c_uint64), ("total_mc_sweeps", C.c_int), ("cell_capacity", C.c_int),
         ("npt_max_dlnV", D), ("volume_moves_per_sweep", C.c_int), ("precision_mode", C.c_int),
         ("init_orientation_cone_deg", D), ("n_read", C.c_int), ("missing_mask", C.c_int),
+        ("energy_check_interval", C.c_int), ("energy_check_tolerance", D), ("init_lattice", C.c_int),
     ]
 
     def as_dict(self):
@@ -46,6 +48,8 @@ class Stats(C.Structure):
         ("volume_attempted", C.c_int64), ("volume_accepted", C.c_int64), ("energy", D), ("box", D * 3),
         ("last_recompute", D), ("drift", D), ("pairs_in_cutoff", C.c_int64), ("stencil_candidates", C.c_int64),
         ("error_flags", C.c_int), ("kernel", C.c_int), ("volume_stage1_rejected", C.c_int64),
+        ("fp64_cells", C.c_int64), ("overcap_cells", C.c_int64), ("energy_checks", C.c_int64),
+        ("drift_breaches", C.c_int64), ("drift_bound", D), ("abs_dE_since_check", D),
     ]
 
 
@@ -81,6 +85,10 @@ EXPORTS = {
     "lcmc_order_parameter": ([C.c_void_p, C.c_int, DP, DP, DP], C.c_int),
     "lcmc_last_outcomes": ([C.c_void_p, C.c_int, C.POINTER(C.c_ubyte), C.c_int], C.c_int),
     "lcmc_set_kernel": ([C.c_void_p, C.c_int], C.c_int),
+    "lcmc_clear_error_flags": ([C.c_void_p], C.c_int),
+    "lcmc_energy_check": ([C.c_void_p], C.c_int),
+    "lcmc_record_moves": ([C.c_void_p, C.c_int], C.c_int),
+    "lcmc_get_move_records": ([C.c_void_p, C.c_int, DP, DP, C.c_int], C.c_int),
     "lcmc_strerror": ([C.c_int], C.c_char_p),
     "lcmc_last_error": ([C.c_void_p, C.c_char_p, C.c_size_t], C.c_int),
     "lcmc_abi_version": ([], C.c_int),
@@ -99,6 +107,7 @@ EXPORTS = {
     "lcmc_mlp_get_params": ([C.c_void_p, FP], C.c_int),
     "lcmc_mlp_set_params": ([C.c_void_p, FP], C.c_int),
     "lcmc_gemm_bf16": ([FP, FP, FP, C.c_int, C.c_int, C.c_int], C.c_int),
+    "lcmc_set_wait_limit": ([C.c_uint], C.c_int),
     "lcmc_set_surrogate": ([C.c_void_p, C.c_void_p, C.c_double], C.c_int),
     "lcmc_set_fp32_screen": ([C.c_void_p, C.c_int], C.c_int),
     "lcmc_get_params": ([C.c_void_p, C.c_int, C.POINTER(Params)], C.c_int),

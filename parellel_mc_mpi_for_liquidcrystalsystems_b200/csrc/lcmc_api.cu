@@ -42,7 +42,12 @@ struct lcmc_ctx {
     double *d_cell_e0 = nullptr, *d_cell_e1 = nullptr;
     int *d_cell_n0 = nullptr, *d_cell_n1 = nullptr;
     unsigned long long *d_cell_pairs = nullptr, *d_cell_cands = nullptr;
+    double *d_cell_abs = nullptr;
+    int *d_cell_fp64 = nullptr;
+    int *d_p2c = nullptr, *d_resc_count = nullptr, *d_resc_list = nullptr;
     unsigned char *d_outcome = nullptr;
+    double *d_rec_dE = nullptr, *d_rec_lu = nullptr; // move records (lcmc_record_moves)
+    std::vector<unsigned long long> sweeps; // host mirror of every replica's sweep counter
     double *d_pe0 = nullptr, *d_pe1 = nullptr;
     int *d_phard = nullptr;
     double *d_red = nullptr;
@@ -71,6 +76,8 @@ struct lcmc_ctx {
     int kernel_override = -1;
     int fast_variant = 0;
     int need_amax = 0; // active-cell capacity the capacity rule asks for
+    int tuned_class = -1; // capacity class lcmc_autotune chose (kept while it holds the rule's capacity)
+    bool checks_off = false; // no periodic energy checks (autotune trials)
     int grid_elem = 0, grid_exact = 0, grid_fast = 0, grid_energy = 0, grid_screen = 0;
     bool any_fast = false, any_exact = false, any_npt = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -114,6 +121,8 @@ extern "C" const char *lcmc_strerror(int code)
     case LCMC_EBOX: return "box too small for the cutoff";
     case LCMC_ENODEV: return "no CUDA device";
     case LCMC_EOVERLAP: return "particle inside the colloid";
+    case LCMC_ETIMEOUT: return "bounded wait gave up";
+    case LCMC_EDRIFT: return "running energy out of tolerance at an FP64 energy check";
     default: return "unknown error";
     }
 }
@@ -231,6 +240,10 @@ extern "C" int lcmc_params_load(const char *path, lcmc_params *p)
                 else ok = sscanf(value, "%d", &p->precision_mode);
             } else if (strcmp(name, "init_orientation_cone_deg") == 0)
                 ok = sscanf(value, "%lf", &p->init_orientation_cone_deg);
+            else if (strcmp(name, "energy_check_interval") == 0) ok = sscanf(value, "%d", &p->energy_check_interval);
+            else if (strcmp(name, "energy_check_tolerance") == 0)
+                ok = sscanf(value, "%lf", &p->energy_check_tolerance);
+            else if (strcmp(name, "init_lattice") == 0) ok = sscanf(value, "%d", &p->init_lattice);
             break; // other keys: ignored, as the reference only warns (MCnptColloid.c:4093)
         }
         if (ok != 1) {
@@ -286,6 +299,10 @@ static void make_consts(const lcmc_params &p, GBConsts &k)
     k.f_4eps0 = (float)k.four_eps0;
     k.f_half_chi = (float)(0.5 * k.chi);
     k.f_half_chip = (float)(0.5 * k.chi_prime);
+    // 25 (4 eps0) = 100 eps0: an FP32 term of that size has a rounding error
+    // of at most ~0.02 eps0 (1.9e-4 relative); larger terms (overlaps) are
+    // evaluated in FP64
+    k.f_big = (float)(25.0 * k.four_eps0);
 }
 
 static double min_cell_width(const lcmc_params &p)
@@ -341,36 +358,77 @@ extern "C" int lcmc_lattice(const lcmc_params *pp, int replica, double *px, doub
         double r2 = xs + ys + zs;
         return R > 0.0 && r2 <= R * R;
     };
-    int ns = 2;
-    for (;; ns++) {
-        long long free_sites = 0;
-        double d = L / (double)ns;
-        for (long long s = 0; s < (long long)ns * ns * ns; s++) {
-            double x = (double)(s % ns) * d, y = (double)((s / ns) % ns) * d, z = (double)(s / ((long long)ns * ns)) * d;
-            if (!inside(x, y, z)) free_sites++;
-        }
-        if (free_sites >= n) break;
-    }
-    const double delta = L / (double)ns;
     uint32_t key[2];
+    if (p.init_lattice == 1) {
+        // body-centred tetragonal: layers c = L / floor(L / (1.05 sigma_ee)) apart
+        // along z, square sites a = L / n_a apart in x, y, the second site of
+        // each cell at (a/2, a/2, c/2); the smallest n_a whose sites outside
+        // the colloid hold N, and the surplus sites left empty evenly over the
+        // site order (site s is kept when floor((s+1) N / S) > floor(s N / S))
+        const double cz = 1.05 * p.gb_sigma_sidetoside * p.gb_kappa;
+        const long long nz = std::max(1LL, (long long)floor(L / cz));
+        const double c = L / (double)nz;
+        auto site = [&](long long s, long long na, double *x, double *y, double *z) {
+            const double a = L / (double)na;
+            const long long b = s & 1, q = s >> 1;
+            const long long ix = q % na, iy = (q / na) % na, iz = q / (na * na);
+            *x = ((double)ix + 0.5 * (double)b) * a;
+            *y = ((double)iy + 0.5 * (double)b) * a;
+            *z = ((double)iz + 0.5 * (double)b) * c;
+        };
+        long long na = 1;
+        std::vector<long long> freeidx;
+        for (;; na++) {
+            freeidx.clear();
+            const long long S = 2 * na * na * nz;
+            for (long long s = 0; s < S; s++) {
+                double x, y, z;
+                site(s, na, &x, &y, &z);
+                if (!inside(x, y, z)) freeidx.push_back(s);
+            }
+            if ((long long)freeidx.size() >= n) break;
+        }
+        const long long F = (long long)freeidx.size();
+        int i = 0;
+        for (long long f = 0; f < F && i < n; f++) {
+            if ((f + 1) * n / F == f * n / F) continue;
+            site(freeidx[f], na, &px[i], &py[i], &pz[i]);
+            i++;
+        }
+    } else {
+        int ns = 2;
+        for (;; ns++) {
+            long long free_sites = 0;
+            double d = L / (double)ns;
+            for (long long s = 0; s < (long long)ns * ns * ns; s++) {
+                double x = (double)(s % ns) * d, y = (double)((s / ns) % ns) * d,
+                       z = (double)(s / ((long long)ns * ns)) * d;
+                if (!inside(x, y, z)) free_sites++;
+            }
+            if (free_sites >= n) break;
+        }
+        const double delta = L / (double)ns;
+        long long site = 0;
+        for (int i = 0; i < n; i++) {
+            double x, y, z;
+            for (;;) {
+                long long ix = site % ns, iy = (site / ns) % ns, iz = site / ((long long)ns * ns);
+                site++;
+                x = (double)ix * delta;
+                y = (double)iy * delta;
+                z = (double)iz * delta;
+                if (!inside(x, y, z)) break;
+            }
+            px[i] = x;
+            py[i] = y;
+            pz[i] = z;
+        }
+    }
     (void)replica;
     seed_key(p.rng_seed, key);
     const double cone = p.init_orientation_cone_deg;
     const double cmin = cos(cone * (pi / 180.0));
-    long long site = 0;
     for (int i = 0; i < n; i++) {
-        double x, y, z;
-        for (;;) {
-            long long ix = site % ns, iy = (site / ns) % ns, iz = site / ((long long)ns * ns);
-            site++;
-            x = (double)ix * delta;
-            y = (double)iy * delta;
-            z = (double)iz * delta;
-            if (!inside(x, y, z)) break;
-        }
-        px[i] = x;
-        py[i] = y;
-        pz[i] = z;
         if (cone >= 180.0) {
             double v[3];
             sphere_point(key, (uint32_t)i, INIT_SWEEP, v);
@@ -433,6 +491,13 @@ static DevView view(const lcmc_ctx *c, int parity)
     v.cell_n1 = c->d_cell_n1;
     v.cell_pairs = c->d_cell_pairs;
     v.cell_cands = c->d_cell_cands;
+    v.cell_abs = c->d_cell_abs;
+    v.cell_fp64 = c->d_cell_fp64;
+    v.p2c = c->d_p2c;
+    v.resc_count = c->d_resc_count;
+    v.resc_list = c->d_resc_list;
+    v.rec_dE = c->d_rec_dE;
+    v.rec_lu = c->d_rec_lu;
     v.outcome = c->d_outcome;
     v.scratch_d = c->d_red;
     v.red_part = c->d_red_part;
@@ -472,7 +537,8 @@ static void free_ctx(lcmc_ctx *c)
     void *ptrs[] = {c->d_rep, c->d_stats, c->d_act_off, c->d_p2r, c->d_id[0], c->d_id[1], c->d_cid, c->d_rank,
                     c->d_perm, c->d_scid, c->d_cell_count, c->d_cell_start, c->d_block_sums, c->d_flag, c->d_cell_e0,
                     c->d_cell_e1, c->d_cell_n0, c->d_cell_n1, c->d_cell_pairs, c->d_cell_cands, c->d_outcome,
-                    c->d_pe0, c->d_pe1, c->d_phard, c->d_red, c->d_red_part};
+                    c->d_pe0, c->d_pe1, c->d_phard, c->d_red, c->d_red_part, c->d_cell_abs, c->d_cell_fp64,
+                    c->d_rec_dE, c->d_rec_lu, c->d_p2c, c->d_resc_count, c->d_resc_list};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int k = 0; k < 8; k++)
@@ -522,8 +588,16 @@ static int lattice_fullest_cell(const lcmc_params &p, double L, double wmin)
     const int nc = grid_dim_host(L, wmin);
     const double V = L * L * L;
     const double vcol = (4.0 / 3.0) * 3.1415926535898 * std::pow(p.colloid_radius, 3);
-    const int ns = (int)std::ceil(std::cbrt(p.num_particles / std::max(1e-3, 1.0 - vcol / V)) - 1e-9);
-    const int per_axis = (int)std::floor((L / (double)nc) * ns / L) + 1;
+    const double nfree = p.num_particles / std::max(1e-3, 1.0 - vcol / V);
+    const double w = L / (double)nc;
+    if (p.init_lattice == 1) { // two interleaved a x a x c sublattices
+        const double nz = std::max(1.0, std::floor(L / (1.05 * p.gb_sigma_sidetoside * p.gb_kappa)));
+        const double na = std::ceil(std::sqrt(nfree / (2.0 * nz)) - 1e-9);
+        const int pxy = (int)std::floor(w * na / L) + 1, pz = (int)std::floor(w * nz / L) + 1;
+        return 2 * pxy * pxy * pz;
+    }
+    const int ns = (int)std::ceil(std::cbrt(nfree) - 1e-9);
+    const int per_axis = (int)std::floor(w * ns / L) + 1;
     return per_axis * per_axis * per_axis;
 }
 
@@ -569,6 +643,37 @@ extern "C" int lcmc_cell_capacity(const lcmc_params *p, int *capacity, int *clas
     return LCMC_OK;
 }
 
+// Per-replica fields that follow from the kernel choice: the FP32 kernel's
+// cell capacity (cells above it are attempted in FP64) and the automatic
+// tolerance of the periodic energy check.
+static void set_caps(lcmc_ctx *c)
+{
+    const int amax = fast_variant(c->fast_variant >> 1).amax;
+    for (int r = 0; r < c->R; r++) {
+        Replica &rp = c->rep[r];
+        const lcmc_params &p = c->params[r];
+        rp.cap = p.cell_capacity > 0 ? std::min(p.cell_capacity, amax) : amax;
+        rp.check_tol = p.energy_check_tolerance > 0.0 ? p.energy_check_tolerance : (rp.kernel == 1 ? 1e-6 : 1e-9);
+    }
+}
+
+// The fields set_caps and choose_kernels write, into the device table.
+static int push_kernel_fields(lcmc_ctx *c)
+{
+    for (int r = 0; r < c->R; r++) {
+        char *base = (char *)c->d_rep + sizeof(Replica) * r;
+        const Replica &rp = c->rep[r];
+        CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, kernel), &rp.kernel, sizeof(int), cudaMemcpyHostToDevice,
+                                    c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, cap), &rp.cap, sizeof(int), cudaMemcpyHostToDevice,
+                                    c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(base + offsetof(Replica, check_tol), &rp.check_tol, sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return LCMC_OK;
+}
+
 // Kernel selection: FP32 kernel for precision_mode fp32 (boxes with >= 4
 // cells per axis; smaller boxes run the FP64 kernel), FP64 kernel otherwise.
 static void choose_kernels(lcmc_ctx *c)
@@ -601,7 +706,10 @@ static void choose_kernels(lcmc_ctx *c)
         spec21 = spec21 && p.gb_mu_exponent == 2.0 && p.gb_nu_exponent == 1.0 && p.gb_sigma_sidetoside == 1.0;
     }
     c->need_amax = need_amax;
-    c->fast_variant = 2 * capacity_class(need_amax) + (spec21 ? 1 : 0);
+    int cls = capacity_class(need_amax);
+    if (c->tuned_class >= 0 && fast_variant(c->tuned_class).amax >= need_amax) cls = c->tuned_class;
+    c->fast_variant = 2 * cls + (spec21 ? 1 : 0);
+    set_caps(c);
 }
 
 static int upload_replica_table(lcmc_ctx *c)
@@ -646,6 +754,8 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
         rp.min_thick = (double)(float)std::min(p.gb_sigma_sidetoside * p.gb_kappa, p.gb_sigma_sidetoside);
         seed_key(p.rng_seed, rp.key);
         make_consts(p, rp.k);
+        rp.check_every = p.energy_check_interval > 0 ? p.energy_check_interval : 0;
+        rp.check_tol = p.energy_check_tolerance; // 0: set by choose_kernels from the kernel
         const double L = box_length(p);
         rp.L[0] = rp.L[1] = rp.L[2] = L;
         if (L < 2.0 * p.cutoff_radius) {
@@ -702,6 +812,11 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     ALLOC(c->d_cell_n1, c->ctot);
     ALLOC(c->d_cell_pairs, c->ctot);
     ALLOC(c->d_cell_cands, c->ctot);
+    ALLOC(c->d_cell_abs, c->ctot);
+    ALLOC(c->d_cell_fp64, c->ctot);
+    ALLOC(c->d_p2c, c->ctot);
+    ALLOC(c->d_resc_count, 8);
+    ALLOC(c->d_resc_list, (size_t)8 * c->ctot);
     ALLOC(c->d_outcome, c->ntot);
     ALLOC(c->d_pe0, c->ntot);
     ALLOC(c->d_pe1, c->ntot);
@@ -713,7 +828,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
             nmax = std::max(nmax, std::max(params[r].num_particles, c->rep[r].nc_max * c->rep[r].nc_max * c->rep[r].nc_max));
         c->red_nchunk = (nmax + LCMC_RED_CHUNK - 1) / LCMC_RED_CHUNK;
     }
-    ALLOC(c->d_red_part, (size_t)n * c->red_nchunk * 6);
+    ALLOC(c->d_red_part, (size_t)n * c->red_nchunk * LCMC_RED_K);
     for (int k = 0; k < 8; k++) ALLOC(c->d_trial_d[k], c->ntot);
     for (int k = 0; k < 3; k++) ALLOC(c->d_trial_f[k], c->ntot);
     ALLOC(c->d_thard, c->ntot);
@@ -730,6 +845,11 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     for (int r = 0; r < n; r++)
         for (int i = 0; i < c->rep[r].n; i++) p2r[c->rep[r].p_off + i] = r;
     cudaMemcpy(c->d_p2r, p2r.data(), sizeof(int) * c->ntot, cudaMemcpyHostToDevice);
+    std::vector<int> p2c(c->ctot);
+    for (int r = 0; r < n; r++)
+        for (int i = 0; i < c->rep[r].nc_max * c->rep[r].nc_max * c->rep[r].nc_max; i++) p2c[c->rep[r].cell_off + i] = r;
+    cudaMemcpy(c->d_p2c, p2c.data(), sizeof(int) * c->ctot, cudaMemcpyHostToDevice);
+    cudaMemset(c->d_resc_count, 0, sizeof(int) * 8);
     cudaMemset(c->d_stats, 0, sizeof(DevStats) * n);
     cudaMemset(c->d_outcome, 0, c->ntot);
     cudaMemset(c->d_cell_e0, 0, sizeof(double) * c->ctot);
@@ -737,6 +857,9 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     cudaMemset(c->d_cell_n1, 0, sizeof(int) * c->ctot);
     cudaMemset(c->d_cell_pairs, 0, sizeof(unsigned long long) * c->ctot);
     cudaMemset(c->d_cell_cands, 0, sizeof(unsigned long long) * c->ctot);
+    cudaMemset(c->d_cell_abs, 0, sizeof(double) * c->ctot);
+    cudaMemset(c->d_cell_fp64, 0, sizeof(int) * c->ctot);
+    c->sweeps.assign(n, 0ull);
     choose_kernels(c);
     c->grid_elem = 4 * c->sms;
     c->grid_exact = 4 * c->sms;
@@ -768,17 +891,31 @@ extern "C" int lcmc_destroy(lcmc_ctx *ctx)
 
 extern "C" int lcmc_num_replicas(const lcmc_ctx *ctx) { return ctx ? ctx->R : 0; }
 
+// Re-run the kernel choice on the replicas' current boxes (read back from the
+// device: NPT volume moves change them) and push the fields it sets.
+static int rechoose_kernels(lcmc_ctx *c)
+{
+    std::vector<Replica> dev(c->R);
+    CUDA_TRY(c, cudaMemcpyAsync(dev.data(), c->d_rep, sizeof(Replica) * c->R, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (int r = 0; r < c->R; r++)
+        for (int a = 0; a < 3; a++) c->rep[r].L[a] = dev[r].L[a];
+    const int old_variant = c->fast_variant;
+    const bool old_fast = c->any_fast, old_exact = c->any_exact;
+    choose_kernels(c);
+    int rc = push_kernel_fields(c);
+    if (rc) return rc;
+    c->grid_fast = fast_blocks_per_sm(c->fast_variant) * c->sms;
+    if (old_variant != c->fast_variant || old_fast != c->any_fast || old_exact != c->any_exact) invalidate_graphs(c);
+    return LCMC_OK;
+}
+
 extern "C" int lcmc_set_kernel(lcmc_ctx *ctx, int kernel)
 {
     if (!ctx || kernel < -1 || kernel > 1) return LCMC_EINVAL;
     ctx->kernel_override = kernel;
-    choose_kernels(ctx);
-    // the device table keeps the dynamic fields; only `kernel` changes
-    for (int r = 0; r < ctx->R; r++)
-        CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * r + offsetof(Replica, kernel),
-                                      &ctx->rep[r].kernel, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    ctx->grid_fast = fast_blocks_per_sm(ctx->fast_variant) * ctx->sms;
+    int rc = rechoose_kernels(ctx);
+    if (rc) return rc;
     invalidate_graphs(ctx);
     return LCMC_OK;
 }
@@ -802,9 +939,13 @@ static void enqueue_sweep(lcmc_ctx *c, int parity)
     DevView v = view(c, parity ^ 1);
     for (int ci = 0; ci < 8; ci++) {
         if (c->any_exact) launch_phase_exact(v, c->stream, ci, c->grid_exact);
-        if (c->any_fast) launch_phase_fast(c->fast_variant, v, c->stream, ci, c->grid_fast);
+        if (c->any_fast) {
+            launch_phase_fast(c->fast_variant, v, c->stream, ci, c->grid_fast);
+            launch_phase_rescue(c->fast_variant & 1, v, c->stream, ci, c->sms);
+        }
     }
     cudaEventRecordWithFlags(c->ev[2], c->stream, cudaEventRecordExternal);
+    launch_sweep_stats(v, c->stream);
     if (c->any_npt) {
         launch_volume_propose(v, c->stream);
         if (c->any_da || c->rec_cap > 0)
@@ -819,7 +960,7 @@ static void enqueue_sweep(lcmc_ctx *c, int parity)
         launch_volume_finish(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, c->grid_energy);
     }
     cudaEventRecordWithFlags(c->ev[3], c->stream, cudaEventRecordExternal);
-    launch_finalize(v, c->stream);
+    launch_sweep_advance(v, c->stream);
     if (c->hist_cap > 0) launch_hist_record(v, c->stream);
     cudaEventRecordWithFlags(c->ev[4], c->stream, cudaEventRecordExternal);
 }
@@ -833,6 +974,90 @@ static int check_flags(lcmc_ctx *c)
     for (auto &s : st) f |= s.flags;
     if (f & (F_CELLCAP | F_STENCILCAP | F_LISTCAP)) return set_err(c, LCMC_ECELLCAP, "cell capacity exceeded");
     if (f & F_NONFINITE) return set_err(c, LCMC_ENUMERIC, "non-finite energy change");
+    if (f & F_DRIFT) {
+        char b[200];
+        for (int r = 0; r < c->R; r++)
+            if (st[r].flags & F_DRIFT) {
+                snprintf(b, sizeof(b), "replica %d: running energy off the FP64 recompute by %.6g (tolerance %.6g)", r,
+                         st[r].drift, st[r].drift_bound);
+                break;
+            }
+        return set_err(c, LCMC_EDRIFT, b);
+    }
+    return LCMC_OK;
+}
+
+// FP64 energy check of the replicas marked in the check kernel (all = every
+// replica; else those whose sweep counter is a multiple of their
+// energy_check_interval): rebin, FP64 total energy, compare and reset.
+static void enqueue_energy_check(lcmc_ctx *c, int all)
+{
+    enqueue_rebin(c, c->cur);
+    c->cur ^= 1;
+    DevView v = view(c, c->cur);
+    launch_energy_exact(v, c->stream, c->d_pe0, c->d_pe1, c->d_phard, 0, c->grid_energy);
+    launch_energy_check(v, c->stream, c->d_pe0, all);
+}
+
+static bool check_due(const lcmc_ctx *c)
+{
+    for (int r = 0; r < c->R; r++) {
+        const int every = c->rep[r].check_every;
+        if (every > 0 && c->sweeps[r] % (unsigned long long)every == 0ull) return true;
+    }
+    return false;
+}
+
+extern "C" int lcmc_energy_check(lcmc_ctx *ctx)
+{
+    if (!ctx) return LCMC_EINVAL;
+    for (int r = 0; r < ctx->R; r++)
+        if (!ctx->uploaded[r]) return set_err(ctx, LCMC_EINVAL, "replica has no configuration (upload or init first)");
+    enqueue_energy_check(ctx, 1);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaGetLastError());
+    return check_flags(ctx);
+}
+
+extern "C" int lcmc_clear_error_flags(lcmc_ctx *ctx)
+{
+    if (!ctx) return LCMC_EINVAL;
+    for (int r = 0; r < ctx->R; r++) {
+        const int zero = 0;
+        CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_stats + sizeof(DevStats) * r + offsetof(DevStats, flags), &zero,
+                                      sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->err.clear();
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_record_moves(lcmc_ctx *ctx, int on)
+{
+    if (!ctx) return LCMC_EINVAL;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (on && !ctx->d_rec_dE) {
+        CUDA_TRY(ctx, dalloc(&ctx->d_rec_dE, ctx->ntot));
+        CUDA_TRY(ctx, dalloc(&ctx->d_rec_lu, ctx->ntot));
+        CUDA_TRY(ctx, cudaMemset(ctx->d_rec_dE, 0, sizeof(double) * ctx->ntot));
+        CUDA_TRY(ctx, cudaMemset(ctx->d_rec_lu, 0, sizeof(double) * ctx->ntot));
+    } else if (!on && ctx->d_rec_dE) {
+        cudaFree(ctx->d_rec_dE);
+        cudaFree(ctx->d_rec_lu);
+        ctx->d_rec_dE = ctx->d_rec_lu = nullptr;
+    }
+    invalidate_graphs(ctx); // the view the graphs captured changed
+    return LCMC_OK;
+}
+
+extern "C" int lcmc_get_move_records(lcmc_ctx *ctx, int replica, double *dE, double *log_u, int n)
+{
+    if (!ctx || replica < 0 || replica >= ctx->R || !dE || !log_u || n != ctx->rep[replica].n) return LCMC_EINVAL;
+    if (!ctx->d_rec_dE) return set_err(ctx, LCMC_EINVAL, "move recording is off (lcmc_record_moves)");
+    const size_t off = (size_t)ctx->rep[replica].p_off;
+    CUDA_TRY(ctx, cudaMemcpyAsync(dE, ctx->d_rec_dE + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(log_u, ctx->d_rec_lu + off, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return LCMC_OK;
 }
 
@@ -858,6 +1083,8 @@ extern "C" int lcmc_sweep(lcmc_ctx *ctx, int n_sweeps)
         CUDA_TRY(ctx, cudaGraphLaunch(ctx->graph[par], ctx->stream));
         ctx->cur = par ^ 1;
         ctx->timed = true;
+        for (int r = 0; r < ctx->R; r++) ctx->sweeps[r]++;
+        if (!ctx->checks_off && check_due(ctx)) enqueue_energy_check(ctx, 0);
     }
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     CUDA_TRY(ctx, cudaGetLastError());
@@ -922,10 +1149,10 @@ extern "C" int lcmc_get_stream(lcmc_ctx *ctx, void **stream)
 extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
 {
     if (!ctx) return LCMC_EINVAL;
-    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases; volume: propose, energy, chunk sums, accept,
-    // scale; surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1; recording; history: chunk sums,
-    // rows; finalize: chunk sums, statistics
-    int n = 8 + 8 * ((int)ctx->any_exact + (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 2;
+    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases (FP32: with the FP64 hand-over kernel); statistics: chunk sums, sums; volume: propose,
+    // energy, chunk sums, accept, scale; surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1;
+    // recording; history: chunk sums, rows; sweep counter
+    int n = 8 + 8 * ((int)ctx->any_exact + 2 * (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 3;
     if (ctx->any_npt && (ctx->any_da || ctx->rec_cap > 0)) n += 2;
     if (ctx->any_npt && ctx->any_da) n += 6;
     if (ctx->any_npt && ctx->any_screen) n += 3; // screen energies, chunk sums, stage 1
@@ -1099,6 +1326,7 @@ extern "C" int lcmc_set_sweep_counter(lcmc_ctx *ctx, int replica, int64_t sweep)
     if (!ctx || replica < 0 || replica >= ctx->R || sweep < 0) return LCMC_EINVAL;
     Replica &rp = ctx->rep[replica];
     rp.sweep = (unsigned long long)sweep;
+    ctx->sweeps[replica] = rp.sweep;
     CUDA_TRY(ctx, cudaMemcpyAsync((char *)ctx->d_rep + sizeof(Replica) * replica + offsetof(Replica, sweep), &rp.sweep,
                                   sizeof(rp.sweep), cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1183,7 +1411,8 @@ static int upload_state(lcmc_ctx *ctx, int replica, const double *px, const doub
                                   sizeof(double) * 3, cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->uploaded[replica] = 1;
-    return LCMC_OK;
+    // the kernel choice and the FP32 kernel's capacity follow the new box
+    return rechoose_kernels(ctx);
 }
 
 extern "C" int lcmc_upload(lcmc_ctx *ctx, int replica, const double *px, const double *py, const double *pz,
@@ -1281,6 +1510,12 @@ extern "C" int lcmc_get_stats(lcmc_ctx *ctx, int replica, lcmc_stats *out)
     out->error_flags = s.flags;
     out->volume_stage1_rejected = (int64_t)s.vol_s1rej;
     out->kernel = rp.use_fast;
+    out->fp64_cells = (int64_t)s.fp64_cells;
+    out->overcap_cells = (int64_t)s.overcap_cells;
+    out->energy_checks = (int64_t)s.checks;
+    out->drift_breaches = (int64_t)s.breaches;
+    out->drift_bound = s.drift_bound;
+    out->abs_dE_since_check = s.abs_dE;
     return LCMC_OK;
 }
 
@@ -1421,6 +1656,10 @@ void tune_cache_append(const char *path, const std::string &key, const TuneChoic
 static int apply_tuning(lcmc_ctx *c, const TuneChoice &ch)
 {
     c->fast_variant = 2 * ch.variant_class + (c->fast_variant & 1);
+    c->tuned_class = ch.variant_class;
+    set_caps(c);
+    int prc = push_kernel_fields(c);
+    if (prc) return prc;
     c->grid_fast = fast_blocks_per_sm(c->fast_variant) * c->sms;
     for (int r = 0; r < c->R; r++) {
         Replica &rp = c->rep[r];
@@ -1519,6 +1758,8 @@ extern "C" int lcmc_autotune(lcmc_ctx *ctx, int sweeps, const char *cache_path, 
             release();
             return set_err(ctx, LCMC_ECUDA, "autotune snapshot");
         }
+        const std::vector<unsigned long long> saved_sweeps = ctx->sweeps;
+        ctx->checks_off = true;
         best_ms = -1.0;
         int rc = LCMC_OK;
         for (const TuneChoice &ch : cand) {
@@ -1536,7 +1777,9 @@ extern "C" int lcmc_autotune(lcmc_ctx *ctx, int sweeps, const char *cache_path, 
                     ms = t / sweeps;
             }
             res.trials++;
+            ctx->sweeps = saved_sweeps;
             if (copy_state(false) != cudaSuccess) {
+                ctx->checks_off = false;
                 release();
                 return set_err(ctx, LCMC_ECUDA, "autotune restore");
             }
@@ -1548,6 +1791,7 @@ extern "C" int lcmc_autotune(lcmc_ctx *ctx, int sweeps, const char *cache_path, 
             }
         }
         release();
+        ctx->checks_off = false;
         if (rc) return rc;
         if (best_ms < 0.0) return set_err(ctx, LCMC_ECELLCAP, "no candidate ran");
         rc = apply_tuning(ctx, best);

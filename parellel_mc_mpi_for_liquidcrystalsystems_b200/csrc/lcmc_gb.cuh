@@ -103,6 +103,31 @@ __device__ __forceinline__ double pair_energy64(const GBConsts &k, double r2, co
     return k.four_eps0 * (ctep1 * ctep2) * erre6 * (erre6 - 1.0);
 }
 
+// pair_energy64 for mu = 2, nu = 1, sigma0 = 1 (no general powers): the FP32
+// kernel's FP64 fallback for cells with overlapping pairs.
+__device__ __forceinline__ double pair_energy64_21(const GBConsts &k, double r2, const double dr[3], const double ei[3],
+                                                   const double ej[3])
+{
+    const double irij = rsqrt(r2);
+    const double rij = r2 * irij;
+    const double iei = rsqrt(ei[0] * ei[0] + ei[1] * ei[1] + ei[2] * ei[2]);
+    const double iej = rsqrt(ej[0] * ej[0] + ej[1] * ej[1] + ej[2] * ej[2]);
+    const double c = iei * iej * (ei[0] * ej[0] + ei[1] * ej[1] + ei[2] * ej[2]);
+    const double a = irij * iei * (dr[0] * ei[0] + dr[1] * ei[1] + dr[2] * ei[2]);
+    const double b = irij * iej * (dr[0] * ej[0] + dr[1] * ej[1] + dr[2] * ej[2]);
+    const double sp2 = (a + b) * (a + b), sm2 = (a - b) * (a - b);
+    const double eps1 = rsqrt(1.0 - k.chi_sq * c * c);
+    const double wp = k.chi_prime * c, wc = k.chi * c;
+    const double eps2 = 1.0 - 0.5 * k.chi_prime * (sp2 * (1.0 - wp) + sm2 * (1.0 + wp)) / (1.0 - wp * wp);
+    const double s_chi = 1.0 - 0.5 * k.chi * (sp2 * (1.0 - wc) + sm2 * (1.0 + wc)) / (1.0 - wc * wc);
+    const double distreal = rij - rsqrt(s_chi) + 1.0;
+    if (distreal < 0.001) return 1000000000.0; // MCnptColloid.c:2670
+    const double erre = 1.0 / distreal;
+    const double erre2 = erre * erre;
+    const double erre6 = erre2 * erre2 * erre2;
+    return k.four_eps0 * (eps1 * eps2 * eps2) * erre6 * (erre6 - 1.0);
+}
+
 // GBCollRod (MCnptColloid.c:1758-1854): colloid of radius R at the box centre.
 __device__ __forceinline__ double colloid_rod(const GBConsts &k, const double ri[3], const double ei[3],
                                               const double L[3])
@@ -148,6 +173,7 @@ __device__ __forceinline__ double colloid_rod(const GBConsts &k, const double ri
 // ---------------------------------------------------------------------------
 struct FastK {
     float rc2, chi, chi_sq, chip, chip_sq, sigma0, four_eps0, half_chi, half_chip;
+    float big; // largest pair-term magnitude the FP32 kernel keeps (larger: the cell runs in FP64)
     int mu_code, nu_code;
     float mu, nu;
 };
@@ -191,6 +217,7 @@ __device__ __forceinline__ FastK fast_consts(const GBConsts &k)
     K.four_eps0 = k.f_4eps0;
     K.half_chi = k.f_half_chi;
     K.half_chip = k.f_half_chip;
+    K.big = k.f_big;
     K.mu_code = k.mu_code;
     K.nu_code = k.nu_code;
     K.mu = (float)k.mu;

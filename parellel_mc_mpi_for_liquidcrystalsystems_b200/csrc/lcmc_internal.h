@@ -12,6 +12,9 @@ struct GBConsts {
     int coll_on;
     int mu_code, nu_code; // 1 or 2: exact integer power; 0: general pow
     float f_rc2, f_chi, f_chi_sq, f_chip, f_chip_sq, f_sigma0, f_4eps0, f_half_chi, f_half_chip;
+    // FP32 kernel: a cell with any pair term above f_big in magnitude (or the
+    // overlap clamp, or a non-finite term) is attempted in FP64 instead
+    float f_big;
 };
 
 // One replica (system).  Static fields are set by the host at create time;
@@ -50,6 +53,12 @@ struct Replica {
     double da_scale;   // surrogate output -> dU / N
     double vol_dU_sur; // surrogate dU of this sweep's move
     int vol_cells;     // 1: the volume move's exact energies by the per-cell kernel (>= 4 cells per axis)
+    int cap;           // FP32 kernel: cells holding more particles are attempted in FP64 (the caller's
+                       // cell_capacity, else the kernel class's capacity)
+    // periodic FP64 energy check: every check_every sweeps (0 = off), tolerance
+    // check_tol relative to max(|E|, N 4 eps0) + sum of |dE| accepted since the last check
+    int check_every;
+    double check_tol;
 };
 
 constexpr int LCMC_FEAT = 8 * 512 + 1; // surrogate input: 8 channels x 8^3 cells + delta ln V
@@ -60,14 +69,21 @@ struct DevStats {
     double energy, last_recompute, drift;
     int flags;
     int pad;
+    unsigned long long fp64_cells;   // FP32-kernel cells attempted in FP64 (large terms or capacity)
+    unsigned long long overcap_cells; // of which: above the cell, stencil or list capacity
+    unsigned long long checks, breaches; // periodic energy checks run / out of tolerance
+    double abs_dE;                   // sum of |dE| of accepted moves since the last check
+    double drift_bound;              // tolerance of the last check
 };
 
 // error flag bits (mirrors LCMC_F_* in lcmc.h)
-constexpr int F_CELLCAP = 1, F_STENCILCAP = 2, F_LISTCAP = 4, F_NONFINITE = 8, F_GRIDCAP = 16;
+constexpr int F_CELLCAP = 1, F_STENCILCAP = 2, F_LISTCAP = 4, F_NONFINITE = 8, F_GRIDCAP = 16, F_DRIFT = 32;
 
 // Launch view of the device buffers, passed by value to every kernel.
 // particles per chunk of the two-level reductions (sums over a replica)
 constexpr int LCMC_RED_CHUNK = 4096;
+// values per chunk in red_part (sums of up to LCMC_RED_K quantities at once)
+constexpr int LCMC_RED_K = 8;
 
 struct DevView {
     int R;              // replicas
@@ -93,9 +109,15 @@ struct DevView {
     double *cell_e0, *cell_e1; // per-cell FP64 sums (sweep dE / energies)
     int *cell_n0, *cell_n1;    // per-cell counts (accepted / hard-core)
     unsigned long long *cell_pairs, *cell_cands;
+    double *cell_abs;          // per cell: sum of |dE| of the accepted moves
+    int *p2c;                  // [ctot] replica of each cell slot
+    int *resc_count;           // [8] cells the FP32 kernel handed over to the FP64 kernel, per colour phase
+    int *resc_list;            // [8 x ctot] their codes: cell * 4 + mode (1 large term, 2 capacity)
+    int *cell_fp64;            // per cell: 0 FP32, 1 attempted in FP64 (large term), 2 (capacity)
     unsigned char *outcome;    // [ntot] by particle slot of id: 0/1/2
+    double *rec_dE, *rec_lu;   // [ntot] by particle slot of id: dE and log u of the last sweep (null: off)
     double *scratch_d;         // [R * 8] small reductions
-    double *red_part;          // [R x red_nchunk x 6] per-chunk partial sums
+    double *red_part;          // [R x red_nchunk x LCMC_RED_K] per-chunk partial sums
     int red_nchunk;            // chunks of LCMC_RED_CHUNK particles per replica (largest replica)
     // this sweep's trial moves, by sorted slot (FP32 kernel systems)
     double *tnx, *tny, *tnz;   // new position, wrapped

@@ -8,7 +8,10 @@ namespace lcmc {
 
 // lcmc_rebin.cu
 void launch_rebin(const DevView &v, cudaStream_t s, int grid);
-void launch_finalize(const DevView &v, cudaStream_t s);
+// per-cell results of the colour phases into the statistics and the running
+// energy (before the volume move); then the sweep counter and adaptive step
+void launch_sweep_stats(const DevView &v, cudaStream_t s);
+void launch_sweep_advance(const DevView &v, cudaStream_t s);
 
 // lcmc_sweep_exact.cu (FP64, bit-identical to the CPU oracle)
 void launch_phase_exact(const DevView &v, cudaStream_t s, int ci, int grid);
@@ -22,6 +25,8 @@ struct FastVariant {
 int fast_variant_count();
 FastVariant fast_variant(int i);
 void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, int grid);
+// FP64 attempts of the cells the FP32 kernel handed over in colour phase ci
+void launch_phase_rescue(bool spec21, const DevView &v, cudaStream_t s, int ci, int grid);
 int fast_blocks_per_sm(int variant);
 
 // lcmc_misc.cu
@@ -32,6 +37,8 @@ void launch_chunk_sums_volume(const DevView &v, cudaStream_t s, const double *e0
 void launch_screen(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid, bool spec21);
 int screen_blocks_per_sm();
 void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, int replica_only);
+// FP64 energy check of the due replicas (all = every replica) from per-particle energies e0
+void launch_energy_check(const DevView &v, cudaStream_t s, const double *e0, int all);
 void launch_volume(const DevView &v, cudaStream_t s, double *e0, double *e1, int *hard, int grid);
 void launch_order_sums(const DevView &v, cudaStream_t s, int r, double *out);
 void launch_to_id_order(const DevView &v, cudaStream_t s, int r, int grid);

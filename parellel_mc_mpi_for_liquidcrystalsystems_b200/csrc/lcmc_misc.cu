@@ -10,7 +10,7 @@ namespace lcmc {
 
 // Two-level sums over a replica's particles, in a fixed order (results repeat
 // bit for bit): blocks (chunk c, replica r) add LCMC_RED_CHUNK particles each
-// into red_part[(r * red_nchunk + c) * 6 + k], then one block per replica adds
+// into red_part[(r * red_nchunk + c) * LCMC_RED_K + k], then one block per replica adds
 // its chunks.  One block streaming a whole replica was limited to one SM's
 // bandwidth (1.9 ms for 8 MB at N = 2^20).
 //   mode 0: k = 0 sum of e0 (total energy)
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(256) k_chunk_sums(DevView v, const double *e0,
     __shared__ double sh[K][8];
     block_sums<K>(s, sh);
     if (threadIdx.x == 0)
-        for (int k = 0; k < K; k++) v.red_part[((size_t)r * v.red_nchunk + c) * 6 + k] = s[k];
+        for (int k = 0; k < K; k++) v.red_part[((size_t)r * v.red_nchunk + c) * LCMC_RED_K + k] = s[k];
 }
 
 // Block per replica: total energy from the chunk sums.  Resets the running
@@ -69,6 +69,45 @@ __global__ void __launch_bounds__(256) k_energy_reduce(DevView v, int replica_on
         st.drift = st.energy - tot;
         st.energy = tot;
         st.last_recompute = tot;
+        st.abs_dE = 0.0;
+        v.scratch_d[r] = tot;
+    }
+}
+
+// Periodic FP64 energy check (EnergyCheck, MCnptColloid.c:1343-1362, called
+// every statistics interval at 946-955, where it prints the running and the
+// recomputed energies): block per replica, the recomputed total from the chunk
+// sums; for replicas that are due (all = 1: every replica; else those whose
+// sweep counter is a multiple of check_every) drift = running - recomputed
+// against the tolerance
+//   check_tol (max(|E|, N 4 eps0) + sum of |dE| accepted since the last check)
+// (the running sum's rounding grows with the energy changes it carried, which
+// near overlaps are many orders above |E|); a breach sets F_DRIFT.  The
+// running energy is reset to the recomputed value either way.
+__global__ void __launch_bounds__(256) k_energy_check(DevView v, int all)
+{
+    const int r = blockIdx.x;
+    const Replica &p = v.rep[r];
+    const bool due = all || (p.check_every > 0 && p.sweep % (unsigned long long)p.check_every == 0ull);
+    if (!due) return;
+    double s[1];
+    finish_sums<1>(v, r, s);
+    if (threadIdx.x == 0) {
+        const double tot = s[0];
+        DevStats &st = v.stats[r];
+        const double drift = st.energy - tot;
+        const double bound = p.check_tol * (fmax(fabs(tot), (double)p.n * p.k.four_eps0) + st.abs_dE);
+        const bool breach = !(fabs(drift) <= bound);
+        st.drift = drift;
+        st.drift_bound = bound;
+        st.checks += 1ull;
+        if (breach) {
+            st.breaches += 1ull;
+            st.flags |= F_DRIFT;
+        }
+        st.energy = tot;
+        st.last_recompute = tot;
+        st.abs_dE = 0.0;
         v.scratch_d[r] = tot;
     }
 }
@@ -113,7 +152,16 @@ __global__ void __launch_bounds__(256) k_volume_accept(DevView v)
         const double U0 = su[0], U1 = su[1];
         const bool H = su[2] > 0.0;
         DevStats &st = v.stats[r];
+        // the exact U(V) doubles as an energy check of the running energy
+        // (same tolerance as the periodic check)
         st.drift = st.energy - U0;
+        st.drift_bound = p.check_tol * (fmax(fabs(U0), (double)p.n * p.k.four_eps0) + st.abs_dE);
+        st.checks += 1ull;
+        if (!(fabs(st.drift) <= st.drift_bound)) {
+            st.breaches += 1ull;
+            st.flags |= F_DRIFT;
+        }
+        st.abs_dE = 0.0;
         st.last_recompute = U0;
         st.vol_att += 1ull;
         p.vol_U_old = U0;
@@ -214,6 +262,12 @@ void launch_energy_reduce(const DevView &v, cudaStream_t s, const double *e0, in
 {
     k_chunk_sums<1, 0><<<chunk_grid(v), 256, 0, s>>>(v, e0, nullptr, nullptr);
     k_energy_reduce<<<v.R, 256, 0, s>>>(v, replica_only);
+}
+
+void launch_energy_check(const DevView &v, cudaStream_t s, const double *e0, int all)
+{
+    k_chunk_sums<1, 0><<<chunk_grid(v), 256, 0, s>>>(v, e0, nullptr, nullptr);
+    k_energy_check<<<v.R, 256, 0, s>>>(v, all);
 }
 
 void launch_chunk_sums_volume(const DevView &v, cudaStream_t s, const double *e0, const double *e1, const int *hard)

@@ -34,10 +34,13 @@ using bf16 = __nv_bfloat16;
 // timeout the tile sets *err and frees its TMEM.
 // ---------------------------------------------------------------------------
 constexpr int GT_M = 128, GT_N = 128, GT_K = 64;
+// mbarrier tries before a wait gives up (lcmc_set_wait_limit lowers it for tests)
+constexpr uint32_t kWaitIters = 1u << 24;
+static uint32_t g_wait_iters = kWaitIters;
 
 __global__ void __launch_bounds__(128) k_gemm_tc(const bf16 *__restrict__ A, int lda, const bf16 *__restrict__ B,
                                                  int ldb, float *__restrict__ C, int ldc, int M, int N, int K,
-                                                 int accumulate, int *err)
+                                                 int accumulate, int *err, uint32_t wait_iters)
 {
     __shared__ __align__(1024) unsigned char sA[GT_M * GT_K * 2];
     __shared__ __align__(1024) unsigned char sB[GT_N * GT_K * 2];
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16 *__restrict__ A, int
             }
             tc::mma_commit(&bar);
         }
-        if (!tc::mbar_wait_bounded(&bar, phase, 1u << 24)) failed = 1;
+        if (!tc::mbar_wait_bounded(&bar, phase, wait_iters)) failed = 1;
         phase ^= 1u;
         __syncthreads();
         if (failed) break;
@@ -113,7 +116,9 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16 *__restrict__ A, int
         }
     } else {
         if (t == 0) atomicOr(err, 1);
-        tc::mbar_wait_bounded(&bar, phase ^ 1u, 1u << 24); // the commit in flight, bounded
+        // the commit in flight (always the full bound, so the MMAs are done
+        // before their TMEM is freed)
+        tc::mbar_wait_bounded(&bar, phase ^ 1u, kWaitIters);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -124,8 +129,23 @@ void gemm_tc(const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, 
              int *err, cudaStream_t s)
 {
     dim3 g((M + GT_M - 1) / GT_M, (N + GT_N - 1) / GT_N);
-    k_gemm_tc<<<g, 128, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate, err);
+    k_gemm_tc<<<g, 128, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate, err, g_wait_iters);
 }
+
+} // namespace lcmc
+
+// Limit of the tensor-core kernels' bounded mbarrier waits, in tries, for
+// launches made from now on (0 restores the default).  A wait that runs out
+// sets the kernel's error flag, drains the MMAs in flight with the full bound,
+// frees its TMEM and returns; the call reports LCMC_ETIMEOUT.  For tests of
+// that path: a limit of 1 makes the first wait give up.
+extern "C" int lcmc_set_wait_limit(unsigned int tries)
+{
+    lcmc::g_wait_iters = tries ? (uint32_t)tries : lcmc::kWaitIters;
+    return LCMC_OK;
+}
+
+namespace lcmc {
 
 // ---------------------------------------------------------------------------
 // MLP kernels (FP32 CUDA cores)

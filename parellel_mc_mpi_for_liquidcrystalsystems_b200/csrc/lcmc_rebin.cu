@@ -65,6 +65,7 @@ __global__ void k_sweep_setup(DevView v)
     __syncthreads();
     if (threadIdx.x < 8) {
         int ci = threadIdx.x;
+        v.resc_count[ci] = 0;
         int *off = v.act_off + ci * (v.R + 1);
         int acc = 0;
         for (int r = 0; r < v.R; r++) {
@@ -269,8 +270,10 @@ __global__ void k_gather(DevView v)
 }
 
 // Per-cell results of a sweep in chunks of LCMC_RED_CHUNK cells (blocks:
-// chunk, replica): dE, accepted, hard-core rejections, in-cutoff pairs and
-// stencil candidates (counts are exact in FP64).
+// chunk, replica): dE, accepted, hard-core rejections, in-cutoff pairs,
+// stencil candidates, sum of |dE| accepted, cells attempted in FP64 by the
+// FP32 kernel and, of those, cells above its capacity (counts are exact in
+// FP64).
 __global__ void __launch_bounds__(256) k_cell_chunk_sums(DevView v)
 {
     const int c = blockIdx.x, r = blockIdx.y;
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(256) k_cell_chunk_sums(DevView v)
     const int i0 = c * LCMC_RED_CHUNK;
     if (i0 >= ncell) return;
     const int i1 = min(ncell, i0 + LCMC_RED_CHUNK);
-    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double s[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (int i = i0 + (int)threadIdx.x; i < i1; i += blockDim.x) {
         const int g = p.cell_off + i;
         s[0] += v.cell_e0[g];
@@ -287,20 +290,27 @@ __global__ void __launch_bounds__(256) k_cell_chunk_sums(DevView v)
         s[2] += (double)v.cell_n1[g];
         s[3] += (double)v.cell_pairs[g];
         s[4] += (double)v.cell_cands[g];
+        s[5] += v.cell_abs[g];
+        const int m = v.cell_fp64[g];
+        s[6] += m != 0 ? 1.0 : 0.0;
+        s[7] += m == 2 ? 1.0 : 0.0;
     }
-    __shared__ double sh[5][8];
-    block_sums<5>(s, sh);
+    __shared__ double sh[8][8];
+    block_sums<8>(s, sh);
     if (threadIdx.x == 0)
-        for (int k = 0; k < 5; k++) v.red_part[((size_t)r * v.red_nchunk + c) * 6 + k] = s[k];
+        for (int k = 0; k < 8; k++) v.red_part[((size_t)r * v.red_nchunk + c) * LCMC_RED_K + k] = s[k];
 }
 
-// Block per replica: add the chunk sums into the statistics, count the sweep.
-__global__ void __launch_bounds__(256) k_sweep_finalize(DevView v)
+// Block per replica: add the chunk sums of the colour phases into the
+// statistics and the running energy.  Runs before the volume move, whose exact
+// U(V) is the energy of the configuration the phases left (the running energy
+// must include their dE when the move compares or replaces it).
+__global__ void __launch_bounds__(256) k_sweep_stats(DevView v)
 {
     const int r = blockIdx.x;
     Replica &p = v.rep[r];
-    double s[5];
-    finish_sums<5>(v, r, p.nc[0] * p.nc[1] * p.nc[2], s);
+    double s[8];
+    finish_sums<8>(v, r, p.nc[0] * p.nc[1] * p.nc[2], s);
     if (threadIdx.x == 0) {
         DevStats &st = v.stats[r];
         st.attempted += (unsigned long long)p.n;
@@ -308,16 +318,28 @@ __global__ void __launch_bounds__(256) k_sweep_finalize(DevView v)
         st.hard += (unsigned long long)s[2];
         st.pairs += (unsigned long long)s[3];
         st.cands += (unsigned long long)s[4];
+        st.abs_dE += s[5];
+        st.fp64_cells += (unsigned long long)s[6];
+        st.overcap_cells += (unsigned long long)s[7];
         st.energy += s[0];
         if (!(s[0] == s[0]) || s[0] - s[0] != 0.0) st.flags |= F_NONFINITE;
+        p.adapt_att += p.adapt_on ? (unsigned long long)p.n : 0ull;
+        p.adapt_acc += p.adapt_on ? (unsigned long long)s[1] : 0ull;
+    }
+}
+
+// One thread per replica, after the volume move (which draws from this
+// sweep's counter): count the sweep, and the adaptive step.
+__global__ void k_sweep_advance(DevView v)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < v.R; r += gridDim.x * blockDim.x) {
+        Replica &p = v.rep[r];
         p.sweep += 1ull;
         // adaptive step (MCnptColloid.c:987-1031) per block of >= 10,000
         // attempts: -5 % below 30 % acceptance, +5 % above 55 %, with the
         // reference's resets at 1e-4 and 1.5 min_thick; never above the cap the
         // cell grid was built for (the checkerboard needs width >= rc + d)
         if (p.adapt_on) {
-            p.adapt_att += (unsigned long long)p.n;
-            p.adapt_acc += (unsigned long long)s[1];
             if (p.adapt_att >= 10000ull) {
                 const double ratio = (double)p.adapt_acc / (double)p.adapt_att;
                 p.adapt_att = 0ull;
@@ -363,10 +385,15 @@ void launch_rebin(const DevView &v, cudaStream_t s, int grid)
     k_gather<<<grid, 256, 0, s>>>(v);
 }
 
-void launch_finalize(const DevView &v, cudaStream_t s)
+void launch_sweep_stats(const DevView &v, cudaStream_t s)
 {
     k_cell_chunk_sums<<<dim3(v.red_nchunk, v.R), 256, 0, s>>>(v);
-    k_sweep_finalize<<<v.R, 256, 0, s>>>(v);
+    k_sweep_stats<<<v.R, 256, 0, s>>>(v);
+}
+
+void launch_sweep_advance(const DevView &v, cudaStream_t s)
+{
+    k_sweep_advance<<<(v.R + 127) / 128, 128, 0, s>>>(v);
 }
 
 } // namespace lcmc

@@ -38,7 +38,7 @@ __device__ __forceinline__ void finish_sums(const DevView &v, int r, int count, 
 #pragma unroll
     for (int k = 0; k < K; k++) s[k] = 0.0;
     for (int c = threadIdx.x; c < nc; c += blockDim.x)
-        for (int k = 0; k < K; k++) s[k] += v.red_part[((size_t)r * v.red_nchunk + c) * 6 + k];
+        for (int k = 0; k < K; k++) s[k] += v.red_part[((size_t)r * v.red_nchunk + c) * LCMC_RED_K + k];
     __shared__ double sh[K][8];
     block_sums<K>(s, sh);
 }

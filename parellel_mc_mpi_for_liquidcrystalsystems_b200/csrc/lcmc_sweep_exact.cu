@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
         __syncwarp();
 
         const int cs = v.cell_start[cell], ce = v.cell_start[cell + 1];
-        double dE_sum = 0.0;
+        double dE_sum = 0.0, dE_abs = 0.0;
         int nacc = 0, nhard = 0;
         unsigned long long npairs = 0ull;
         const unsigned long long cands = (unsigned long long)(s_base[wib][ncell] - 1) * (unsigned long long)(ce - cs);
@@ -102,7 +102,13 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
             double rn[3], en[3], dsp[3], uacc;
             int ok = make_trial(p, id, ro, eo, rn, en, dsp, &uacc);
             if (!ok) {
-                if (lane == 0) v.outcome[p.p_off + id] = 2;
+                if (lane == 0) {
+                    v.outcome[p.p_off + id] = 2;
+                    if (v.rec_dE) {
+                        v.rec_dE[p.p_off + id] = 0.0;
+                        v.rec_lu[p.p_off + id] = log_unit(uacc);
+                    }
+                }
                 nhard++;
                 continue;
             }
@@ -148,9 +154,16 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
                     v.oz[g] = en[2];
                 }
                 dE_sum += dE;
+                dE_abs += fabs(dE);
                 nacc++;
             }
-            if (lane == 0) v.outcome[p.p_off + id] = acc ? 1 : 0;
+            if (lane == 0) {
+                v.outcome[p.p_off + id] = acc ? 1 : 0;
+                if (v.rec_dE) {
+                    v.rec_dE[p.p_off + id] = dE;
+                    v.rec_lu[p.p_off + id] = log_unit(uacc);
+                }
+            }
             __syncwarp();
         }
         // pair counter: sum over lanes
@@ -158,6 +171,8 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
         for (int o = 16; o >= 1; o >>= 1) npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
         if (lane == 0) {
             v.cell_e0[cell] = dE_sum;
+            v.cell_abs[cell] = dE_abs;
+            v.cell_fp64[cell] = 0;
             v.cell_n0[cell] = nacc;
             v.cell_n1[cell] = nhard;
             v.cell_pairs[cell] = npairs;

@@ -47,6 +47,19 @@
 //   6 decide   warp 0: Metropolis decisions in id order (fixed-point passes
 //              over the triangular system the sequential order defines)
 //   7 write    accepted trial states to the FP64 master arrays
+//
+// FP64 fallback per cell: FP32 rounding of a pair term is relative to the
+// term, and near an overlap (R^12 up to 1e36 just above the 1e9 clamp) it
+// exceeds any energy scale, so a decision or a running energy built from such
+// terms is meaningless.  A cell in which any FP32 pair term (static or
+// in-cell, old or new state) exceeds f_big in magnitude, hits the overlap
+// clamp or is not finite makes no move here and is handed over to
+// k_phase_rescue, which attempts it from the same phase-start state in FP64
+// (every thread of a block over the 27 stencil cells' particles, read from the
+// FP64 master arrays, on the one-fold minimum image), and so is a cell above
+// the kernel's capacity (particles, staged candidates or list entries).  Below f_big the FP32 terms carry an
+// absolute error of at most about 2e-4 f_big / 100 (1.9e-4 relative, stated
+// per pair), so decisions differ from FP64 only at near-ties.
 #include <cuda_runtime.h>
 
 #include "lcmc_gb.cuh"
@@ -92,19 +105,19 @@ struct FastSmem {
     int segcnt[NW];
     int task;
     int overflow;
+    int big; // a pair term above f_big (or clamped, or non-finite): attempt the cell in FP64
     unsigned long long pairs;
 };
 
-
-__device__ __forceinline__ void cell_failed(const DevView &v, int r, int cell, int flag)
+// Hand a cell over to the FP64 phase kernel (k_phase_rescue, launched after
+// this one in the same colour phase); it writes the cell's results.
+__device__ __forceinline__ void hand_over(const DevView &v, int ci, int cell, int mode)
 {
-    atomicOr(&v.stats[r].flags, flag);
-    v.cell_e0[cell] = 0.0;
-    v.cell_n0[cell] = 0;
-    v.cell_n1[cell] = 0;
-    v.cell_pairs[cell] = 0ull;
-    v.cell_cands[cell] = 0ull;
+    const int i = atomicAdd(&v.resc_count[ci], 1);
+    v.resc_list[(size_t)ci * v.ctot + i] = cell * 4 + mode;
 }
+
+
 
 // resident CTAs per SM the register budget is sized for: the 48-particle
 // class (36.9 KB of shared memory) fits six per SM at 80 registers, the
@@ -155,6 +168,7 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
         }
         if (t == 0) {
             sm.overflow = 0;
+            sm.big = 0;
             sm.pairs = 0ull;
             sm.task = 0;
         }
@@ -174,9 +188,8 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
         const int na = sm.st_cnt[13];
         const int g0 = sm.st_start[13];
         const int S26 = sm.st_pre[27];
-        if (na > AMAX) {
-            if (t == 0) cell_failed(v, r, cell, F_CELLCAP);
-            for (int k = t; k < na; k += NT) v.outcome[p.p_off + v.id[g0 + k]] = 0;
+        if (na > AMAX || na > p.cap) { // above capacity: the whole cell in FP64
+            if (t == 0) hand_over(v, ci, cell, 2);
             __syncthreads();
             continue;
         }
@@ -262,9 +275,8 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
             }
         }
         __syncthreads();
-        if (sm.overflow) {
-            if (t == 0) cell_failed(v, r, cell, F_STENCILCAP);
-            for (int k = t; k < na; k += NT) v.outcome[p.p_off + v.id[g0 + k]] = 0;
+        if (sm.overflow) { // staged candidates above a warp segment's capacity
+            if (t == 0) hand_over(v, ci, cell, 2);
             __syncthreads();
             continue;
         }
@@ -276,7 +288,7 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
         unsigned long long npairs = 0ull;
         for (;;) {
             int task = 0;
-            if (lane == 0) task = atomicAdd(&sm.task, 1);
+            if (lane == 0) task = *(volatile int *)&sm.big ? ntask : atomicAdd(&sm.task, 1);
             task = __shfl_sync(0xffffffffu, task, 0);
             if (task >= ntask) break;
             if (task < nptask) {
@@ -349,6 +361,7 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                         r2 = dx * dx + dy * dy + dz * dz;
                         const float e1 = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, P2.y, P2.z, P2.w, c.w, u.x, u.y);
                         const bool in1 = r2 < K.rc2;
+                        if ((in0 && !(fabsf(e0) <= K.big)) || (in1 && !(fabsf(e1) <= K.big))) sm.big = 1;
                         const double d0 = in0 ? (double)e0 : 0.0, d1 = in1 ? (double)e1 : 0.0;
                         if (isa) {
                             soa += d0;
@@ -417,7 +430,9 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                         D = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, R2.y, R2.z, R2.w, Q2.y, Q2.z, Q2.w);
                         D = r2 < K.rc2 ? D : 0.0f;
                     }
-                    // differences in FP64 (exact cancellation of the overlap clamp), then rounded
+                    if (!(fabsf(A) <= K.big && fabsf(B) <= K.big && fabsf(Cc) <= K.big && fabsf(D) <= K.big))
+                        sm.big = 1;
+                    // differences in FP64, then rounded (each term is at most f_big here)
                     const double a = A, b = B, c = Cc, d = D;
                     sm.pCA[idx] = (float)(c - a);
                     sm.pBA[idx] = (float)(b - a);
@@ -430,9 +445,8 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
         }
         if (lane == 0 && npairs) atomicAdd(&sm.pairs, npairs);
         __syncthreads();
-        if (sm.overflow) {
-            if (t == 0) cell_failed(v, r, cell, F_LISTCAP);
-            for (int k = t; k < na; k += NT) v.outcome[p.p_off + v.id[g0 + k]] = 0;
+        if (sm.overflow || sm.big) { // list capacity exceeded, or a term FP32 cannot carry
+            if (t == 0) hand_over(v, ci, cell, sm.overflow ? 2 : 1);
             __syncthreads();
             continue;
         }
@@ -507,14 +521,30 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
             }
             if (v0) sm.acc[lane] = (acc0 >> lane) & 1u;
             if (v1) sm.acc[lane + 32] = (acc1 >> lane) & 1u;
+            if (v.rec_dE) {
+                if (v0) {
+                    v.rec_dE[p.p_off + sm.pid[lane]] = ((hd0 >> lane) & 1u) ? 0.0 : x0;
+                    v.rec_lu[p.p_off + sm.pid[lane]] = lu0;
+                }
+                if (v1) {
+                    v.rec_dE[p.p_off + sm.pid[lane + 32]] = ((hd1 >> lane) & 1u) ? 0.0 : x1;
+                    v.rec_lu[p.p_off + sm.pid[lane + 32]] = lu1;
+                }
+            }
             // accepted dE summed in a fixed (butterfly) order
             double dsum = ((acc0 >> lane) & 1u ? x0 : 0.0) + ((acc1 >> lane) & 1u ? x1 : 0.0);
+            double dabs = ((acc0 >> lane) & 1u ? fabs(x0) : 0.0) + ((acc1 >> lane) & 1u ? fabs(x1) : 0.0);
 #pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+            for (int o = 16; o >= 1; o >>= 1) {
+                dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+                dabs += __shfl_xor_sync(0xffffffffu, dabs, o);
+            }
             const int nacc = __popc(acc0) + __popc(acc1), nhard = __popc(hd0) + __popc(hd1);
             if (lane == 0) {
                 if (!(dsum - dsum == 0.0)) atomicOr(&v.stats[r].flags, F_NONFINITE);
                 v.cell_e0[cell] = dsum;
+                v.cell_abs[cell] = dabs;
+                v.cell_fp64[cell] = 0;
                 v.cell_n0[cell] = nacc;
                 v.cell_n1[cell] = nhard;
                 v.cell_pairs[cell] = sm.pairs;
@@ -539,6 +569,171 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                 v.cl2[g] = make_float2(P2.z, P2.w);
             }
             v.outcome[p.p_off + sm.pid[k]] = sm.hard[k] ? 2 : acc;
+        }
+        __syncthreads();
+    }
+}
+
+// FP64 attempts of the cells the FP32 phase kernel handed over in colour phase
+// ci (a pair term above f_big: an overlap, where FP32 rounding of R^12
+// exceeds every energy scale; or a cell above the kernel's capacity), block
+// per cell, sequentially in the in-cell order (ascending id) from the
+// phase-start state, with the trial moves the gather drew (tn*, tu*, tdU, tlu,
+// thard): E_old and E_new of each attempt are sums of the FP64 pair term
+// (pair_exact; its lighter form for mu = 2, nu = 1, sigma0 = 1) over the 27
+// stencil cells' particles read from the FP64 master arrays (earlier accepted
+// in-cell moves already written), one-fold minimum image, every thread of the
+// block over the candidates, then a fixed-order block sum.
+// dE = (E_new - E_old) + dU_colloid, accepted if dE <= 0 or ln u <= -beta dE
+// (MCnptColloid.c:2491-2574).  The FP32 state copy of an accepted particle is
+// written exactly as the FP32 kernel writes it.  No per-particle state in
+// shared memory, so any cell count works.  The other cells of the colour do
+// not interact with these, so running them after the FP32 kernel changes
+// nothing in the chain.
+template <int NT, bool SPEC21>
+__global__ void __launch_bounds__(NT) k_phase_rescue(DevView v, int ci)
+{
+    constexpr int NW = NT / 32;
+    __shared__ int st_start[27], st_cnt[27], pre[28];
+    __shared__ double spo[NW], spn[NW];
+    __shared__ int snp[NW];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int count = v.resc_count[ci];
+    for (int e = blockIdx.x; e < count; e += gridDim.x) {
+        const int code = v.resc_list[(size_t)ci * v.ctot + e];
+        const int cell = code >> 2, mode = code & 3;
+        const int r = v.p2c[cell];
+        const Replica &p = v.rep[r];
+        const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
+        const int loc = cell - p.cell_off;
+        const int cx = loc % nc0, cy = (loc / nc0) % nc1, cz = loc / (nc0 * nc1);
+        if (t < 27) {
+            int x = cx + t % 3 - 1, y = cy + (t / 3) % 3 - 1, z = cz + t / 9 - 1;
+            x += x < 0 ? nc0 : (x >= nc0 ? -nc0 : 0);
+            y += y < 0 ? nc1 : (y >= nc1 ? -nc1 : 0);
+            z += z < 0 ? nc2 : (z >= nc2 ? -nc2 : 0);
+            const int c = p.cell_off + (z * nc1 + y) * nc0 + x;
+            st_start[t] = v.cell_start[c];
+            st_cnt[t] = v.cell_start[c + 1] - v.cell_start[c];
+        }
+        __syncthreads();
+        if (t < 32) {
+            const int c = t < 27 ? st_cnt[t] : 0;
+            int inc = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            if (t < 27) pre[t] = inc - c;
+            if (t == 26) pre[27] = inc;
+        }
+        __syncthreads();
+        const int total = pre[27];
+        const int g0 = st_start[13], na = st_cnt[13];
+        double dsum = 0.0, dabs = 0.0;
+        int nacc = 0, nhard = 0;
+        unsigned long long npairs = 0ull;
+        for (int k = 0; k < na; k++) {
+            const int g = g0 + k;
+            const int id = v.id[g];
+            if (v.thard[g]) { // colloid hard-core reject: no energy evaluation
+                if (t == 0) {
+                    v.outcome[p.p_off + id] = 2;
+                    if (v.rec_dE) {
+                        v.rec_dE[p.p_off + id] = 0.0;
+                        v.rec_lu[p.p_off + id] = v.tlu[g];
+                    }
+                }
+                nhard++;
+                continue;
+            }
+            const double ro[3] = {v.px[g], v.py[g], v.pz[g]};
+            const double eo[3] = {v.ox[g], v.oy[g], v.oz[g]};
+            const double rn[3] = {v.tnx[g], v.tny[g], v.tnz[g]};
+            const double en[3] = {v.tux[g], v.tuy[g], v.tuz[g]};
+            double po = 0.0, pn = 0.0;
+            int np = 0;
+            for (int f = t; f < total; f += NT) {
+                int sl = 0, hi = 27;
+                while (hi - sl > 1) {
+                    const int mid = (sl + hi) >> 1;
+                    if (pre[mid] <= f) sl = mid;
+                    else hi = mid;
+                }
+                const int j = st_start[sl] + (f - pre[sl]);
+                if (j == g) continue;
+                const double rj[3] = {v.px[j], v.py[j], v.pz[j]};
+                const double ej[3] = {v.ox[j], v.oy[j], v.oz[j]};
+                double d[3];
+                double r2 = dist_fold(ro[0], ro[1], ro[2], rj[0], rj[1], rj[2], p.L, d);
+                if (r2 < p.k.rc2) {
+                    po += SPEC21 ? pair_energy64_21(p.k, r2, d, eo, ej) : pair_exact(p.k, r2, d, eo, ej);
+                    np++;
+                }
+                r2 = dist_fold(rn[0], rn[1], rn[2], rj[0], rj[1], rj[2], p.L, d);
+                if (r2 < p.k.rc2) {
+                    pn += SPEC21 ? pair_energy64_21(p.k, r2, d, en, ej) : pair_exact(p.k, r2, d, en, ej);
+                    np++;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) {
+                po += __shfl_xor_sync(0xffffffffu, po, o);
+                pn += __shfl_xor_sync(0xffffffffu, pn, o);
+                np += __shfl_xor_sync(0xffffffffu, np, o);
+            }
+            if (lane == 0) {
+                spo[w] = po;
+                spn[w] = pn;
+                snp[w] = np;
+            }
+            __syncthreads();
+            if (t == 0) {
+                double so = spo[0], sn = spn[0];
+                int sp = snp[0];
+                for (int q = 1; q < NW; q++) {
+                    so += spo[q];
+                    sn += spn[q];
+                    sp += snp[q];
+                }
+                const double dE = (sn - so) + v.tdU[g];
+                const double lu = v.tlu[g];
+                const bool acc = (dE <= 0.0) || (lu <= -p.k.beta * dE);
+                if (acc) {
+                    v.px[g] = rn[0];
+                    v.py[g] = rn[1];
+                    v.pz[g] = rn[2];
+                    v.ox[g] = en[0];
+                    v.oy[g] = en[1];
+                    v.oz[g] = en[2];
+                    const float4 c4 = v.cl4[g];
+                    float tux, tuy, tuz;
+                    unit_f32(en[0], en[1], en[2], tux, tuy, tuz);
+                    v.cl4[g] = make_float4(c4.x + v.tdx[g], c4.y + v.tdy[g], c4.z + v.tdz[g], tux);
+                    v.cl2[g] = make_float2(tuy, tuz);
+                    dsum += dE;
+                    dabs += fabs(dE);
+                    nacc++;
+                }
+                v.outcome[p.p_off + id] = acc ? 1 : 0;
+                if (v.rec_dE) {
+                    v.rec_dE[p.p_off + id] = dE;
+                    v.rec_lu[p.p_off + id] = lu;
+                }
+                npairs += (unsigned long long)sp;
+            }
+            __syncthreads(); // the accepted state is visible to the next attempt
+        }
+        if (t == 0) {
+            if (!(dsum - dsum == 0.0)) atomicOr(&v.stats[r].flags, F_NONFINITE);
+            v.cell_e0[cell] = dsum;
+            v.cell_abs[cell] = dabs;
+            v.cell_n0[cell] = nacc;
+            v.cell_n1[cell] = nhard;
+            v.cell_pairs[cell] = npairs;
+            v.cell_cands[cell] = (unsigned long long)na * (unsigned long long)(total > 0 ? total - 1 : 0);
+            v.cell_fp64[cell] = mode;
         }
         __syncthreads();
     }
@@ -586,6 +781,12 @@ void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, in
     case 4: launch_v<128, 64, 288, 384, false>(v, s, ci, grid); break;
     default: launch_v<128, 64, 288, 384, true>(v, s, ci, grid); break;
     }
+}
+
+void launch_phase_rescue(bool spec21, const DevView &v, cudaStream_t s, int ci, int grid)
+{
+    if (spec21) k_phase_rescue<256, true><<<grid, 256, 0, s>>>(v, ci);
+    else k_phase_rescue<256, false><<<grid, 256, 0, s>>>(v, ci);
 }
 
 // Also opts the variant in to its dynamic shared memory size: call once

@@ -38,8 +38,9 @@ def load_initial_conditions(path, **overrides):
 
 
 def lattice(params, replica=0):
-    """Seeded simple-cubic start (initialize_cubic_lattice_positions,
-    MCnptColloid.c:2920-3033) computed on the host; returns (6 arrays, box)."""
+    """Seeded lattice start (initialize_cubic_lattice_positions,
+    MCnptColloid.c:2920-3033: simple cubic; init_lattice = 1: body-centred
+    tetragonal along z) computed on the host; returns (6 arrays, box)."""
     n = params.num_particles
     a = [np.zeros(n) for _ in range(6)]
     box = np.zeros(3)
@@ -137,6 +138,28 @@ class GBSystem:
     def set_kernel(self, kernel):
         """-1 automatic, 0 the FP64 kernel, 1 the FP32 kernel."""
         self._check(lib().lcmc_set_kernel(self._h, kernel))
+
+    def energy_check(self):
+        """EnergyCheck (MCnptColloid.c:1343-1362) now: FP64 recompute of every
+        replica, drift recorded, running energy reset; raises LcmcError
+        (EDRIFT) when a replica's drift is beyond its tolerance."""
+        self._check(lib().lcmc_energy_check(self._h))
+
+    def clear_error_flags(self):
+        """Clear the sticky error flags (after handling an error)."""
+        self._check(lib().lcmc_clear_error_flags(self._h))
+
+    def record_moves(self, on=True):
+        """Record every attempt's dE and ln u (per particle id) from now on."""
+        self._check(lib().lcmc_record_moves(self._h, int(bool(on))))
+
+    def move_records(self, replica=0):
+        """(dE, ln u) of the last sweep's attempts, by particle id."""
+        n = self.params[replica].num_particles
+        dE, lu = np.zeros(n), np.zeros(n)
+        self._check(lib().lcmc_get_move_records(self._h, replica, dE.ctypes.data_as(_lib.DP),
+                                                lu.ctypes.data_as(_lib.DP), n))
+        return dE, lu
 
     def stats(self, replica=0):
         s = Stats()

@@ -52,3 +52,28 @@ def test_resumed_run_ends_where_one_run_ends(tmp_path):
     lcmc.run_simulation(write_params(two, 0, 4000), two, histogram=False)  # resume from two/fortSphere.1
     a, b = sidecar_state(one / "fortSphere.1"), sidecar_state(two / "fortSphere.1")
     assert a.size == b.size and np.array_equal(a, b)
+
+
+def test_c_host_writes_what_run_simulation_writes(tmp_path):
+    """tests/c_host/lcmc_run.c (the cycle loop in C over include/lcmc.h) and
+    run_simulation, on one parameter file: the same status lines and the same
+    bytes in every output file (Configuraciones.dat, fortSphere.1 and its
+    sidecar, qmga_mcnvtGB.cnf, Histograma_Movimientos.dat)."""
+    import subprocess
+
+    from test_c_host_cpu import build_c_host
+
+    exe = build_c_host(tmp_path / "lcmc_run")
+    c_dir, py_dir = tmp_path / "c", tmp_path / "py"
+    c_dir.mkdir()
+    py_dir.mkdir()
+    params = write_params(tmp_path, 2, 5000)
+    r = subprocess.run([str(exe), str(params), str(c_dir)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = []
+    lcmc.run_simulation(params, py_dir, log=lines.append)
+    c_lines = r.stdout.splitlines()
+    assert c_lines[:-1] == lines and c_lines[-1].startswith("done: 5 sweeps")
+    for name in ("Configuraciones.dat", "fortSphere.1", "fortSphere.1.lcmc", "qmga_mcnvtGB.cnf",
+                 "Histograma_Movimientos.dat"):
+        assert (c_dir / name).read_bytes() == (py_dir / name).read_bytes(), name

@@ -1,0 +1,168 @@
+"""FP32 production kernel against the FP64 kernel at the large-system state
+point (rho* = 0.32, T* = 0.8, orientations within 20 degrees of z), the FP64
+hand-over of overlapping or over-full cells, and the periodic FP64 energy
+check (EnergyCheck, MCnptColloid.c:1343-1362).
+
+Lockstep: an FP32-kernel system and an FP64-kernel system start every sweep
+from the same FP64 state with the same seed and sweep counter, so they draw
+the same trial moves and the same Metropolis numbers; their decisions are
+compared particle by particle, and every attempt's energy change dE is
+compared with the FP64 kernel's.  FP32 pair terms carry at most 1.9e-4
+relative error (max(|phi|, 1)); terms above 100 eps0 are evaluated in FP64, so
+an attempt's FP32 dE differs from FP64 by far less than kT except where
+overlaps make it huge, and decisions differ only where beta dE is within that
+difference of ln u.
+"""
+import numpy as np
+import pytest
+
+import parellel_mc_mpi_for_liquidcrystalsystems_b200 as lcmc
+from parellel_mc_mpi_for_liquidcrystalsystems_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+T = 0.8
+
+
+def params(n, lattice, seed=7, precision=1, **kw):
+    return lcmc.default_params(num_particles=n, system_density=0.32, system_temperature=T, gb_kappa=3.0,
+                               gb_kappa_prime=5.0, gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
+                               max_displacement=0.1, max_rotation=0.1, init_orientation_cone_deg=20.0,
+                               precision_mode=precision, rng_seed=seed, init_lattice=lattice, **kw)
+
+
+def lockstep(n, lattice, sweeps, relax=0):
+    """Per sweep: (outcomes32, outcomes64, dE32, dE64, ln u, fp64 cells so far)."""
+    p = params(n, lattice)
+    st, box = lcmc.lattice(p)
+    rows = []
+    with lcmc.GBSystem(p) as a, lcmc.GBSystem(p) as b:
+        b.set_kernel(0)
+        b.upload(*st, box)
+        if relax:
+            b.sweep(relax)
+        a.record_moves(True)
+        b.record_moves(True)
+        for _ in range(sweeps):
+            x, bx = b.download()
+            a.upload(*x, bx)
+            _lib.check(_lib.lib().lcmc_set_sweep_counter(a._h, 0, b.stats()["sweeps"]))
+            a.sweep(1)
+            b.sweep(1)
+            ea, _ = a.move_records()
+            eb, lu = b.move_records()
+            rows.append((a.outcomes(), b.outcomes(), ea, eb, lu, a.stats()["fp64_cells"]))
+    return rows
+
+
+@pytest.mark.parametrize("lattice,relax", [(0, 0), (1, 40)], ids=["jammed-sc-lattice", "relaxed-bct"])
+def test_fp32_decisions_match_fp64_at_rho032(lattice, relax):
+    """50 lockstep sweeps of N = 32,768: from the simple-cubic lattice start
+    (spacing 1.46 for rods of length 3: overlaps up to the 1e9 clamp and
+    terms of 1e36 beside it) and from a relaxed state."""
+    n = 32768
+    rows = lockstep(n, lattice, 50, relax)
+    for o32, o64, e32, e64, lu, _ in rows:
+        assert np.array_equal(o32 == 2, o64 == 2)  # hard-core rejects need no energy
+        soft = o64 != 2
+        agree = np.mean(o32[soft] == o64[soft])
+        assert agree >= 0.999, agree
+        dd = np.abs(e32 - e64)
+        # FP32 error of an attempt: below 1e-3 kT where |dE| is O(1), and
+        # relative 1e-5 where the FP64 fallback carried large terms
+        assert np.all(dd[soft] <= 1e-3 + 1e-5 * np.abs(e64[soft])), dd[soft].max()
+        # a decision differs only where the FP32 error crosses the acceptance threshold
+        for i in np.nonzero(o32 != o64)[0]:
+            assert abs(e64[i] / T - lu[i]) <= abs(e32[i] - e64[i]) / T + 1e-12
+    if lattice == 0:
+        assert rows[-1][5] > 0  # the overlapping start went through the FP64 hand-over
+
+
+def test_overfull_cells_run_in_fp64():
+    """cell_capacity = 8 at 22 particles per cell: every cell is above the
+    FP32 kernel's capacity and is attempted in FP64 (fail-safe, counted),
+    with the FP64 kernel's decisions."""
+    n = 32768
+    p = params(n, 1, cell_capacity=8)
+    st, box = lcmc.lattice(p)
+    with lcmc.GBSystem(p) as a, lcmc.GBSystem(params(n, 1)) as b:
+        b.set_kernel(0)
+        for s in (a, b):
+            s.upload(*st, box)
+        same = True
+        for _ in range(3):
+            a.sweep(1)
+            b.sweep(1)
+            oa, ob = a.outcomes(), b.outcomes()
+            assert np.mean(oa == ob) >= 0.9999
+            same = same and np.array_equal(oa, ob)
+        sa = a.stats()
+        assert sa["error_flags"] == 0 and sa["kernel"] == 1
+        assert sa["overcap_cells"] == sa["fp64_cells"] > 0
+        if same:  # identical decisions: the same states up to the pair term's last bits
+            ea, eb = a.tot_ene(), b.tot_ene()
+            assert abs(ea - eb) <= 1e-9 * abs(eb)
+
+
+def test_periodic_energy_check_passes_and_resets():
+    """energy_check_interval = 5: four checks in 20 sweeps, none out of
+    tolerance, the running energy equal to the FP64 recompute after each."""
+    n = 32768
+    p = params(n, 1, energy_check_interval=5)
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(20)
+        st = s.stats()
+        assert st["energy_checks"] == 4 and st["drift_breaches"] == 0
+        assert abs(st["drift"]) <= st["drift_bound"]
+        assert st["drift_bound"] > 0.0
+        assert st["energy"] == st["last_recompute"]
+        e = s.tot_ene()
+        assert abs(st["energy"] - e) <= 1e-9 * abs(e)
+
+
+def test_energy_check_flags_a_planted_drift():
+    """A caller that hands over a wrong running energy (the in/out energy of
+    attempt_monte_carlo_move) is caught by the next check: LCMC_EDRIFT, the
+    breach counted, the running energy reset to the recompute; after the
+    caller clears the flags the run goes on."""
+    n = 8192
+    p = params(n, 1, energy_check_interval=2)
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        state, box = s.download()
+        e_true = s.tot_ene()
+        s.upload(*state, box, energy=e_true + 1.0e4)
+        s.sweep(1)  # no check due yet
+        with pytest.raises(lcmc.LcmcError) as ex:
+            s.sweep(1)
+        assert ex.value.code == _lib.EDRIFT
+        st = s.stats()
+        assert st["drift_breaches"] == 1 and st["error_flags"] & _lib.F_DRIFT
+        assert abs(st["drift"] - 1.0e4) < 1.0
+        assert st["energy"] == st["last_recompute"]
+        s.clear_error_flags()
+        s.sweep(4)
+        assert s.stats()["drift_breaches"] == 1
+        # the explicit check agrees
+        s.energy_check()
+        assert s.stats()["drift_breaches"] == 1
+
+
+def test_npt_running_energy_tracks_the_recompute():
+    """NPT: the volume move's exact U(V) is compared with the running energy
+    every sweep (after the colour phases' dE is added), so the running
+    energy equals the FP64 recompute within FP32 rounding."""
+    n = 8192
+    p = lcmc.default_params(num_particles=n, system_density=0.30, system_temperature=0.9, system_pressure=2.0,
+                            mc_ensemble_type=2, npt_max_dlnV=0.01, rng_seed=3, precision_mode=1,
+                            init_orientation_cone_deg=20.0, init_lattice=1, gb_kappa=3.0, gb_kappa_prime=5.0,
+                            gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0, max_displacement=0.1,
+                            max_rotation=0.1)
+    with lcmc.GBSystem(p) as s:
+        s.get_initial_config()
+        s.sweep(30)
+        st = s.stats()
+        assert st["drift_breaches"] == 0 and st["energy_checks"] == 30
+        e = s.tot_ene()
+        assert abs(st["energy"] - e) <= 1e-6 * (abs(e) + n)

@@ -97,3 +97,26 @@ def test_mlp_training_reduces_loss():
         assert loss1 < 0.2 * loss0
     finally:
         L.lcmc_mlp_destroy(h)
+
+
+def test_bounded_wait_gives_up_cleanly():
+    """With the mbarrier wait limit at one try, the GEMM's first wait gives up:
+    the kernel sets its error flag, drains its MMAs (full bound), frees its
+    TMEM and returns, and the call reports LCMC_ETIMEOUT; nothing faults or
+    hangs.  With the default limit back, the next call computes the product."""
+    L = lib()
+    rng = np.random.default_rng(5)
+    M, N, K = 256, 256, 1024
+    a = rng.standard_normal((M, K)).astype(np.float32)
+    b = rng.standard_normal((N, K)).astype(np.float32)
+    c = np.zeros((M, N), dtype=np.float32)
+    try:
+        assert L.lcmc_set_wait_limit(1) == 0
+        assert L.lcmc_gemm_bf16(fp(a), fp(b), fp(c), M, N, K) == _lib.ETIMEOUT
+    finally:
+        L.lcmc_set_wait_limit(0)
+    assert L.lcmc_gemm_bf16(fp(a), fp(b), fp(c), M, N, K) == 0
+    ab = a.astype(np.float64)
+    bb = b.astype(np.float64)
+    want = mo.bf16(ab) @ mo.bf16(bb).T
+    assert np.max(np.abs(c - want)) <= 1e-3 * np.max(np.abs(want))

@@ -45,7 +45,7 @@ def test_library_exports_every_header_symbol():
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
     exported = set(re.findall(r" T (lcmc_\w+)", out))
     assert set(names) <= exported
-    assert lib.lcmc_abi_version() == 1
+    assert lib.lcmc_abi_version() == 2
 
 
 def test_params_parser_matches_oracle(golden):
@@ -127,3 +127,57 @@ def test_cell_capacity_rule(kw, lo, cls):
     cap, klass = C.c_int(), C.c_int()
     assert _lib.lib().lcmc_cell_capacity(C.byref(p), C.byref(cap), C.byref(klass)) == 0
     assert cap.value >= lo and klass.value == cls, (cap.value, klass.value)
+
+
+def _gb_pair_terms(pos, u, L, rmax=3.6):
+    """FP64 numpy restatement of pij_GB (MCnptColloid.c:2618-2681) for
+    GB(3, 5, 2, 1), sigma0 = eps0 = 1, over all pairs closer than rmax
+    (test infrastructure): (terms, distreal)."""
+    import numpy as np
+    from scipy.spatial import cKDTree
+
+    pairs = cKDTree(pos, boxsize=L * (1 + 1e-12)).query_pairs(rmax, output_type="ndarray")
+    i, j = pairs[:, 0], pairs[:, 1]
+    d = pos[j] - pos[i]
+    d -= L * np.round(d / L)
+    r = np.linalg.norm(d, axis=1)
+    rh = d / r[:, None]
+    chi, kp = 0.8, np.sqrt(5.0)
+    chip = (kp - 1) / (kp + 1)
+    a, b, c = (rh * u[i]).sum(1), (rh * u[j]).sum(1), (u[i] * u[j]).sum(1)
+
+    def g(w):
+        return 1 - 0.5 * w * ((a + b) ** 2 / (1 + w * c) + (a - b) ** 2 / (1 - w * c))
+
+    dr = r - 1 / np.sqrt(g(chi)) + 1
+    R = 1 / np.maximum(dr, 1e-3)
+    phi = np.where(dr < 0.001, 1e9, 4 / np.sqrt(1 - chi ** 2 * c ** 2) * g(chip) ** 2 * R ** 6 * (R ** 6 - 1))
+    return phi, dr
+
+
+def test_body_centred_lattice_start_has_no_overlaps():
+    """init_lattice = 1 (host only): N sites of a body-centred tetragonal
+    lattice with layers 1.05 sigma_ee apart along z.  With orientations drawn
+    within 20 degrees of z some tilted neighbours still overlap (about 1 % of
+    pairs above 100 eps0), but no pair is inside the reference's 1e9 clamp or
+    beside it (distreal > 0.2, terms below 1e9), so every overlap relaxes;
+    the simple-cubic start at this density holds clamped pairs."""
+    import numpy as np
+    from parellel_mc_mpi_for_liquidcrystalsystems_b200 import mc
+
+    n = 32768
+    p = mc.default_params(num_particles=n, system_density=0.32, init_orientation_cone_deg=20.0, init_lattice=1,
+                          rng_seed=5)
+    (px, py, pz, ox, oy, oz), box = mc.lattice(p)
+    L = box[0]
+    assert np.all((px >= 0) & (px < L) & (py >= 0) & (py < L) & (pz >= 0) & (pz < L))
+    pos = np.stack([px, py, pz], 1)
+    assert len(np.unique(np.round(pos * 1e6).astype(np.int64), axis=0)) == n
+    assert np.all(oz >= np.cos(np.radians(20.0)) - 1e-12)
+    phi, dr = _gb_pair_terms(pos, np.stack([ox, oy, oz], 1), L)
+    assert dr.min() > 0.2 and phi.max() < 1e9
+    assert np.mean(phi > 100.0) < 0.02
+    p0 = mc.default_params(num_particles=n, system_density=0.32, init_orientation_cone_deg=20.0, rng_seed=5)
+    (qx, qy, qz, ux, uy, uz), box0 = mc.lattice(p0)
+    phi0, dr0 = _gb_pair_terms(np.stack([qx, qy, qz], 1), np.stack([ux, uy, uz], 1), box0[0])
+    assert dr0.min() < 0.001 and phi0.max() >= 1e9
