@@ -16,9 +16,16 @@
 #                                   for bit-exact golden vectors
 #   oracle/_ref/libmcref_omp.so     -O3 -fopenmp: the reference's OpenMP
 #                                   pragmas enabled, used as the timed CPU baseline
+#
+# Usage: build_ref.sh <reference directory>   (or LCMC_REFERENCE_DIR set)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${LCMC_REFERENCE_DIR:-/root/reference}/MCnptColloid.c"
+REFDIR="${1:-${LCMC_REFERENCE_DIR:-}}"
+if [ -z "$REFDIR" ]; then
+    echo "build_ref.sh: give the reference directory (argument or LCMC_REFERENCE_DIR); oracle/_ref not rebuilt" >&2
+    exit 0
+fi
+REF="$REFDIR/MCnptColloid.c"
 OUT="$HERE/_ref"
 if [ ! -f "$REF" ]; then
     echo "build_ref.sh: $REF not found; oracle/_ref not rebuilt" >&2

@@ -247,7 +247,7 @@ def test_fp32_runs_are_deterministic():
             s.sweep(3)
             outs.append(s.download())
             ms = s.last_sweep_timing()  # event nodes inside the sweep graph
-            assert ms[0] > 0 and ms[1] > 0 and ms[3] >= 0 and s.kernels_per_sweep() == 18
+            assert ms[0] > 0 and ms[1] > 0 and ms[3] >= 0 and s.kernels_per_sweep() == 27
     for a, b in zip(outs[0][0], outs[1][0]):
         assert np.array_equal(bits(a), bits(b))
 
