@@ -528,6 +528,89 @@ def jammed_start(lcmc, torch, steps, warmup):
 
 
 # ---------------------------------------------------------------------------
+# batched replicas (64 independent systems of uneven N, T, P, colloid)
+# ---------------------------------------------------------------------------
+def batch_replica_params(lcmc, n_rep=64, seed=2024):
+    """The batch workload: N log-uniform in [4096, 65536], T* uniform on
+    [0.6, 1.4]; even replicas NVT at rho* 0.30-0.34, odd ones NPT at P*
+    1.5-2.5; every third replica with a colloid of R uniform in [3, 6];
+    GB(3, 5, 2, 1), rc = 4, FP32 kernel, fine cell grid (odd cell counts
+    allowed, so small boxes keep cells about one cutoff wide), body-centred
+    lattice starts with orientations within 20 degrees of z."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ps = []
+    for r in range(n_rep):
+        n = int(round(float(np.exp(rng.uniform(np.log(4096), np.log(65536))))))
+        T = float(rng.uniform(0.6, 1.4))
+        rho = float(rng.uniform(0.30, 0.34))
+        npt = r % 2 == 1
+        P = float(rng.uniform(1.5, 2.5))
+        R = float(rng.uniform(3.0, 6.0)) if r % 3 == 0 else 0.0
+        ps.append(lcmc.default_params(
+            num_particles=n, system_density=rho, system_temperature=T, system_pressure=P,
+            mc_ensemble_type=2 if npt else 1, npt_max_dlnV=0.01, colloid_radius=R, colloid_wall_option=1 if R else 0,
+            gb_kappa=3.0, gb_kappa_prime=5.0, gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
+            max_displacement=0.1, max_rotation=0.1, precision_mode=1, cell_grid=1, init_lattice=1,
+            init_orientation_cone_deg=20.0, rng_seed=seed * 1000 + r))
+    return ps
+
+
+def batch_workload(lcmc, torch, steps, warmup, single_rate=None):
+    """Moves/s of the 64-replica batch in one graph-launched sweep (device time
+    per sweep, L2 flushed between sweeps), with the autotuner's choice."""
+    import numpy as np
+    ps = batch_replica_params(lcmc)
+    ntot = sum(p.num_particles for p in ps)
+    s = lcmc.GBSystem(ps)
+    for r in range(len(ps)):
+        s.get_initial_config(r)
+    tune = s.autotune(sweeps=2)
+    s.sweep(max(3, warmup))
+    ext = torch.cuda.ExternalStream(s.stream_handle())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    st0 = [s.stats(r) for r in range(len(ps))]
+    ms, parts = [], []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        s.sweep(1)
+        b.record(ext)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        parts.append(s.last_sweep_timing())
+    st1 = [s.stats(r) for r in range(len(ps))]
+    parts = np.median(np.array(parts), axis=0)
+    fp64_cells = sum(b_["fp64_cells"] - a_["fp64_cells"] for a_, b_ in zip(st0, st1))
+    try:
+        s.energy_check()
+        check_ok = True
+    except lcmc.LcmcError:
+        check_ok = False
+    worst = max(abs(s.stats(r)["drift"]) / max(s.stats(r)["drift_bound"], 1e-300) for r in range(len(ps)))
+    kps = s.kernels_per_sweep()
+    s.close()
+    value = ntot * steps / (sum(ms) * 1e-3)
+    out = {"workload": "64 replicas, N log-uniform in [4096, 65536], T* U[0.6, 1.4], half NVT at rho* 0.30-0.34, "
+                       "half NPT at P* 1.5-2.5, a third with a colloid R U[3, 6]; FP32 kernel, fine cell grid, "
+                       "one CUDA graph per sweep over the replica table",
+           "replicas": len(ps), "n_total": ntot, "n_min": min(p.num_particles for p in ps),
+           "n_max": max(p.num_particles for p in ps), "steps": steps, "warmup": max(3, warmup),
+           "ms_per_step": statistics.mean(ms), "value": value, "unit": UNIT,
+           "replicas_on_fp32_kernel": int(sum(st["kernel"] for st in st1)),
+           "fp64_cells_per_sweep": fp64_cells / steps,
+           "ms_parts_median": {"rebin": parts[0], "colour_phases": parts[1], "stats_and_volume": parts[2],
+                               "advance": parts[3]},
+           "kernels_per_sweep": kps, "autotune": tune,
+           "energy_check": {"ok": check_ok, "max_drift_over_tolerance": worst}}
+    if single_rate:
+        out["per_move_rate_vs_single_system"] = value / single_rate
+    return out
+
+
+# ---------------------------------------------------------------------------
 # ranks: the job's time is the slowest rank's; value = all ranks' units / that
 # ---------------------------------------------------------------------------
 def max_over_ranks(dist, x, device="cuda"):
@@ -567,6 +650,8 @@ def main():
     ap.add_argument("--npt-screen", action="store_true", help="npt workload with the FP32-pair volume screen")
     ap.add_argument("--jammed-steps", type=int, default=5,
                     help="timed sweeps of the simple-cubic (jammed) start sub-measurement (0 skips it)")
+    ap.add_argument("--batch-steps", type=int, default=10,
+                    help="timed sweeps of the 64-replica batch sub-measurement (0 skips it)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -675,6 +760,9 @@ def main():
     jam = None
     if args.jammed_steps > 0 and world == 1:
         jam = jammed_start(lcmc, torch, args.jammed_steps, args.warmup)
+    batch = None
+    if args.batch_steps > 0 and world == 1:
+        batch = batch_workload(lcmc, torch, args.batch_steps, args.warmup, single_rate=value)
 
     if rank != 0:
         if dist:
@@ -724,6 +812,8 @@ def main():
     }
     if jam:
         line["jammed_start"] = jam
+    if batch:
+        line["batch"] = batch
     if clocks:
         line["clocks"] = clocks
     if peaks:

@@ -105,6 +105,11 @@ typedef struct {
                                         reference's), 1 = body-centred tetragonal with the long axis along z,
                                         spacing 1.05 sigma_ee along z (a start for orientations near z
                                         with no pair in the overlap clamp) */
+    int cell_grid;                   /* 0 = even cell count per axis, 8-colour checkerboard (the CPU oracle's
+                                        schedule); 1 = fine: the largest count of cells at least
+                                        cutoff + max_displacement wide, odd counts taking 3 colours on that
+                                        axis (up to 27 colour phases), so small boxes keep cells about one
+                                        cutoff wide (and on the FP32 kernel) instead of up to 1.5 cutoffs */
 } lcmc_params;
 
 typedef struct {
@@ -324,10 +329,11 @@ int lcmc_set_sweep_counter(lcmc_ctx *ctx, int replica, int64_t sweep);
 /* Active-cell capacity the FP32 kernel takes for a system created with *p (no
  * counterpart in the reference, whose cells are unbounded host arrays): the
  * caller's cell_capacity when given; else, from the creation density, the
- * mean occupancy of a cell m plus six standard deviations of its count (variance
- * m for a gas, rho* <= 0.15, and 0.3 m for a dense liquid, rho* >= 0.25) plus 6,
- * at least what the lattice start puts in its fullest cell, and at least 56
- * for NPT.  class_capacity: the kernel class used (48, 56 or 64).  Host only. */
+ * mean occupancy of a cell m plus four standard deviations of its count
+ * (variance m for a gas, rho* <= 0.15, and 0.3 m for a dense liquid,
+ * rho* >= 0.25) plus 4, and at least 56 for NPT.  A cell holding more (a
+ * lattice start's fullest cells, a rare fluctuation) is attempted in FP64.
+ * class_capacity: the kernel class used (48, 56 or 64).  Host only. */
 int lcmc_cell_capacity(const lcmc_params *p, int *capacity, int *class_capacity);
 
 /* Autotuner (no counterpart in the reference): times `sweeps` sweeps (after

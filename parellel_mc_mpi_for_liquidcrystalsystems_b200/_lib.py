@@ -36,6 +36,7 @@ class Params(C.Structure):
         ("npt_max_dlnV", D), ("volume_moves_per_sweep", C.c_int), ("precision_mode", C.c_int),
         ("init_orientation_cone_deg", D), ("n_read", C.c_int), ("missing_mask", C.c_int),
         ("energy_check_interval", C.c_int), ("energy_check_tolerance", D), ("init_lattice", C.c_int),
+        ("cell_grid", C.c_int),
     ]
 
     def as_dict(self):

@@ -45,6 +45,7 @@ struct lcmc_ctx {
     double *d_cell_abs = nullptr;
     int *d_cell_fp64 = nullptr;
     int *d_p2c = nullptr, *d_resc_count = nullptr, *d_resc_list = nullptr;
+    int nphase = 8; // colour phases per sweep (LCMC_MAX_COLOURS with a fine-grid replica)
     unsigned char *d_outcome = nullptr;
     double *d_rec_dE = nullptr, *d_rec_lu = nullptr; // move records (lcmc_record_moves)
     std::vector<unsigned long long> sweeps; // host mirror of every replica's sweep counter
@@ -244,6 +245,7 @@ extern "C" int lcmc_params_load(const char *path, lcmc_params *p)
             else if (strcmp(name, "energy_check_tolerance") == 0)
                 ok = sscanf(value, "%lf", &p->energy_check_tolerance);
             else if (strcmp(name, "init_lattice") == 0) ok = sscanf(value, "%d", &p->init_lattice);
+            else if (strcmp(name, "cell_grid") == 0) ok = sscanf(value, "%d", &p->cell_grid);
             break; // other keys: ignored, as the reference only warns (MCnptColloid.c:4093)
         }
         if (ok != 1) {
@@ -312,10 +314,10 @@ static double min_cell_width(const lcmc_params &p)
     return w;
 }
 
-static int grid_dim_host(double L, double wmin)
+static int grid_dim_host(double L, double wmin, bool fine)
 {
     int m = (int)floor(L / wmin);
-    return m >= 2 ? m - (m & 1) : 1;
+    return m >= 2 ? ((fine && m >= 3) ? m : m - (m & 1)) : 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -495,6 +497,7 @@ static DevView view(const lcmc_ctx *c, int parity)
     v.cell_fp64 = c->d_cell_fp64;
     v.p2c = c->d_p2c;
     v.resc_count = c->d_resc_count;
+    v.nphase = c->nphase;
     v.resc_list = c->d_resc_list;
     v.rec_dE = c->d_rec_dE;
     v.rec_lu = c->d_rec_lu;
@@ -575,38 +578,19 @@ static void invalidate_graphs(lcmc_ctx *c)
 
 // Active-cell capacity the FP32 kernel needs for a system in a cubic box of
 // side L: the caller's cell_capacity when given; else the mean occupancy m
-// plus six standard deviations of a cell's count plus 6, with the variance m S:
-// S = 1 (Poisson) for a gas (rho* <= 0.15), 0.3 for a dense liquid (rho* >= 0.25,
-// whose counts fluctuate far less), linear between; and at least what the
-// lattice start puts in its fullest cell.  NPT systems, whose box may compress
-// far below its creation volume, take at least the middle class.  A cell above
-// the capacity is flagged after the sweep.
-// particles the lattice start puts in its fullest cell: sites a = L / n_s
-// apart, floor(w / a) + 1 per axis
-static int lattice_fullest_cell(const lcmc_params &p, double L, double wmin)
-{
-    const int nc = grid_dim_host(L, wmin);
-    const double V = L * L * L;
-    const double vcol = (4.0 / 3.0) * 3.1415926535898 * std::pow(p.colloid_radius, 3);
-    const double nfree = p.num_particles / std::max(1e-3, 1.0 - vcol / V);
-    const double w = L / (double)nc;
-    if (p.init_lattice == 1) { // two interleaved a x a x c sublattices
-        const double nz = std::max(1.0, std::floor(L / (1.05 * p.gb_sigma_sidetoside * p.gb_kappa)));
-        const double na = std::ceil(std::sqrt(nfree / (2.0 * nz)) - 1e-9);
-        const int pxy = (int)std::floor(w * na / L) + 1, pz = (int)std::floor(w * nz / L) + 1;
-        return 2 * pxy * pxy * pz;
-    }
-    const int ns = (int)std::ceil(std::cbrt(nfree) - 1e-9);
-    const int per_axis = (int)std::floor(w * ns / L) + 1;
-    return per_axis * per_axis * per_axis;
-}
-
+// plus four standard deviations of a cell's count plus 4, with the variance
+// m S: S = 1 (Poisson) for a gas (rho* <= 0.15), 0.3 for a dense liquid
+// (rho* >= 0.25, whose counts fluctuate far less), linear between.  NPT
+// systems, whose box may compress far below its creation volume, take at
+// least the middle class.  A cell above the capacity (a lattice start's
+// fullest cells, a rare fluctuation) is attempted in FP64 by the hand-over
+// kernel.
 // mean occupancy of a cell and the standard deviation of its count (variance
 // m S: S = 1, Poisson, for a gas, rho* <= 0.15; 0.3 for a dense liquid,
 // rho* >= 0.25, whose counts fluctuate far less; linear between)
 static void cell_count_stats(const lcmc_params &p, double L, double wmin, double *mean, double *sd)
 {
-    const int nc = grid_dim_host(L, wmin);
+    const int nc = grid_dim_host(L, wmin, p.cell_grid == 1);
     const double rho = p.num_particles / (L * L * L);
     const double wcell = L / (double)nc;
     const double S = rho >= 0.25 ? 0.3 : (rho <= 0.15 ? 1.0 : 1.0 - 0.7 * (rho - 0.15) / 0.10);
@@ -619,8 +603,10 @@ static int capacity_rule(const lcmc_params &p, double L, double wmin, bool npt)
     if (p.cell_capacity > 0) return p.cell_capacity;
     double mean, sd;
     cell_count_stats(p, L, wmin, &mean, &sd);
-    int want = (int)std::ceil(mean + 6.0 * sd + 6.0);
-    want = std::max(want, lattice_fullest_cell(p, L, wmin));
+    // a cell above the capacity is attempted in FP64 (correct, only slower),
+    // so the rule sizes for the liquid, not for the lattice start's fullest
+    // cells or rare fluctuations: 4 standard deviations, + 4
+    int want = (int)std::ceil(mean + 4.0 * sd + 4.0);
     if (npt) want = std::max(want, fast_variant(1).amax);
     return want;
 }
@@ -693,7 +679,7 @@ static void choose_kernels(lcmc_ctx *c)
             capacity_rule(p, rp.L[0], rp.wmin, rp.ensemble == 2) > fast_variant(fast_variant_count() - 1).amax)
             kern = 0;
         rp.kernel = kern;
-        int nc = grid_dim_host(rp.L[0], rp.wmin);
+        int nc = grid_dim_host(rp.L[0], rp.wmin, rp.fine);
         if (kern == 1) {
             c->any_fast = true;
             if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
@@ -749,6 +735,8 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
         rp.pressure = p.system_pressure;
         rp.dlnv_max = rp.ensemble == 2 && p.volume_moves_per_sweep > 0 ? p.npt_max_dlnV : 0.0;
         rp.wmin = min_cell_width(p);
+        rp.fine = p.cell_grid == 1 ? 1 : 0;
+        if (rp.fine) c->nphase = LCMC_MAX_COLOURS;
         rp.d_cap = (double)p.max_displacement;
         rp.vol_cells = 1;
         rp.min_thick = (double)(float)std::min(p.gb_sigma_sidetoside * p.gb_kappa, p.gb_sigma_sidetoside);
@@ -764,7 +752,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
         }
         // cell grid capacity: NVT boxes keep their size; NPT boxes may grow (then cells stay wider)
         double Lmax = rp.ensemble == 2 ? 1.25 * L : L;
-        rp.nc_max = grid_dim_host(Lmax, rp.wmin);
+        rp.nc_max = grid_dim_host(Lmax, rp.wmin, rp.fine);
         rp.cell_off = coff;
         rp.sweep = 0ull;
         poff += rp.n;
@@ -792,7 +780,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
         }
     ALLOC(c->d_rep, n);
     ALLOC(c->d_stats, n);
-    ALLOC(c->d_act_off, 8 * (n + 1));
+    ALLOC(c->d_act_off, c->nphase * (n + 1));
     ALLOC(c->d_p2r, c->ntot);
     for (int a = 0; a < 2; a++) {
         for (int k = 0; k < 6; k++) ALLOC(c->d_x[a][k], c->ntot);
@@ -815,8 +803,8 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     ALLOC(c->d_cell_abs, c->ctot);
     ALLOC(c->d_cell_fp64, c->ctot);
     ALLOC(c->d_p2c, c->ctot);
-    ALLOC(c->d_resc_count, 8);
-    ALLOC(c->d_resc_list, (size_t)8 * c->ctot);
+    ALLOC(c->d_resc_count, c->nphase);
+    ALLOC(c->d_resc_list, (size_t)c->nphase * c->ctot);
     ALLOC(c->d_outcome, c->ntot);
     ALLOC(c->d_pe0, c->ntot);
     ALLOC(c->d_pe1, c->ntot);
@@ -849,7 +837,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     for (int r = 0; r < n; r++)
         for (int i = 0; i < c->rep[r].nc_max * c->rep[r].nc_max * c->rep[r].nc_max; i++) p2c[c->rep[r].cell_off + i] = r;
     cudaMemcpy(c->d_p2c, p2c.data(), sizeof(int) * c->ctot, cudaMemcpyHostToDevice);
-    cudaMemset(c->d_resc_count, 0, sizeof(int) * 8);
+    cudaMemset(c->d_resc_count, 0, sizeof(int) * c->nphase);
     cudaMemset(c->d_stats, 0, sizeof(DevStats) * n);
     cudaMemset(c->d_outcome, 0, c->ntot);
     cudaMemset(c->d_cell_e0, 0, sizeof(double) * c->ctot);
@@ -937,7 +925,7 @@ static void enqueue_sweep(lcmc_ctx *c, int parity)
     enqueue_rebin(c, parity);
     cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal);
     DevView v = view(c, parity ^ 1);
-    for (int ci = 0; ci < 8; ci++) {
+    for (int ci = 0; ci < c->nphase; ci++) {
         if (c->any_exact) launch_phase_exact(v, c->stream, ci, c->grid_exact);
         if (c->any_fast) {
             launch_phase_fast(c->fast_variant, v, c->stream, ci, c->grid_fast);
@@ -1152,7 +1140,7 @@ extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
     // rebin: setup, bin, 3 scan, scatter, sort, gather; phases (FP32: with the FP64 hand-over kernel); statistics: chunk sums, sums; volume: propose,
     // energy, chunk sums, accept, scale; surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1;
     // recording; history: chunk sums, rows; sweep counter
-    int n = 8 + 8 * ((int)ctx->any_exact + 2 * (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 3;
+    int n = 8 + ctx->nphase * ((int)ctx->any_exact + 2 * (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 3;
     if (ctx->any_npt && (ctx->any_da || ctx->rec_cap > 0)) n += 2;
     if (ctx->any_npt && ctx->any_da) n += 6;
     if (ctx->any_npt && ctx->any_screen) n += 3; // screen energies, chunk sums, stage 1
@@ -1693,7 +1681,7 @@ extern "C" int lcmc_autotune(lcmc_ctx *ctx, int sweeps, const char *cache_path, 
         std::vector<TuneChoice> cand;
         bool npt4 = false; // an NPT replica on the per-cell volume kernel's grid (>= 4 cells per axis)
         for (int r = 0; r < ctx->R; r++)
-            npt4 = npt4 || (ctx->rep[r].ensemble == 2 && grid_dim_host(ctx->rep[r].L[0], ctx->rep[r].wmin) >= 4);
+            npt4 = npt4 || (ctx->rep[r].ensemble == 2 && grid_dim_host(ctx->rep[r].L[0], ctx->rep[r].wmin, ctx->rep[r].fine) >= 4);
         for (int v = 0; v < fast_variant_count(); v++) {
             if (!ctx->any_fast && v != (ctx->fast_variant >> 1)) continue;
             // classes below the rule's capacity are not tried (the largest always is)

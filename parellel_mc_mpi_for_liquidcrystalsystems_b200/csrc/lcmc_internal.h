@@ -4,6 +4,21 @@
 
 namespace lcmc {
 
+// Most colour phases of a sweep: 3 colours per axis on odd cell counts (fine grid).
+constexpr int LCMC_MAX_COLOURS = 27;
+
+// Cells of colour b along an axis of nc cells with k colours (k = 2: cells
+// b, b + 2, ...; k = 3, odd nc: 0 and 1 alternate over the first nc - 1 cells
+// and colour 2 is the last cell), and the index of the j-th of them.
+__host__ __device__ __forceinline__ int axis_colour_count(int nc, int k, int b)
+{
+    return k == 3 ? (b == 2 ? 1 : (nc - 1) / 2) : (nc - b + 1) / 2;
+}
+__host__ __device__ __forceinline__ int axis_colour_cell(int nc, int k, int b, int j)
+{
+    return (k == 3 && b == 2) ? nc - 1 : 2 * j + b;
+}
+
 // Derived constants of one system (get_system_const, MCnptColloid.c:2752-2783,
 // with chi computed after kappa^2).  FP64, plus FP32 copies for the FP32 kernel.
 struct GBConsts {
@@ -24,6 +39,7 @@ struct Replica {
     int p_off;    // first particle slot in the concatenated arrays
     int cell_off; // first cell slot
     int nc_max;   // cells per axis allocated (nc_max^3 cells)
+    int fine;     // cell grid: 0 even counts per axis (8 colours), 1 any count (odd: 3 colours on that axis)
     int ensemble; // 1 NVT, 2 NPT
     int kernel;   // 0 FP64 kernel, 1 FP32 kernel
     int npt_energy_fp64;
@@ -35,7 +51,9 @@ struct Replica {
     int nc[3];
     double w[3];
     double shift[3];
-    int perm[8];
+    int kc[3];      // colours per axis: 2 (even count, or 1 cell), 3 (odd count >= 3, fine grid only)
+    int ncol;       // colours this sweep: kc[0] kc[1] kc[2]
+    int perm[LCMC_MAX_COLOURS]; // colour of each phase (-1: phase empty for this replica)
     unsigned long long sweep;
     int use_fast;  // this sweep runs the FP32 kernel (needs >= 4 cells per axis)
     // volume move of this sweep
@@ -91,7 +109,8 @@ struct DevView {
     int ctot;           // cells allocated, all replicas
     Replica *rep;       // [R]
     DevStats *stats;    // [R]
-    int *act_off;       // [8 * (R + 1)] active-cell prefix per phase
+    int *act_off;       // [nphase * (R + 1)] active-cell prefix per phase
+    int nphase;         // colour phases per sweep: 8, or LCMC_MAX_COLOURS with a fine-grid replica
     int *p2r;           // [ntot] replica of each particle slot
     // particle state, cell-sorted (current buffer)
     double *px, *py, *pz, *ox, *oy, *oz;
@@ -111,8 +130,8 @@ struct DevView {
     unsigned long long *cell_pairs, *cell_cands;
     double *cell_abs;          // per cell: sum of |dE| of the accepted moves
     int *p2c;                  // [ctot] replica of each cell slot
-    int *resc_count;           // [8] cells the FP32 kernel handed over to the FP64 kernel, per colour phase
-    int *resc_list;            // [8 x ctot] their codes: cell * 4 + mode (1 large term, 2 capacity)
+    int *resc_count;           // [nphase] cells the FP32 kernel handed over to the FP64 kernel, per colour phase
+    int *resc_list;            // [nphase x ctot] their codes: cell * 4 + mode (1 large term, 2 capacity)
     int *cell_fp64;            // per cell: 0 FP32, 1 attempted in FP64 (large term), 2 (capacity)
     unsigned char *outcome;    // [ntot] by particle slot of id: 0/1/2
     double *rec_dE, *rec_lu;   // [ntot] by particle slot of id: dE and log u of the last sweep (null: off)

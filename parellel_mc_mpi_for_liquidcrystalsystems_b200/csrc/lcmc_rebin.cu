@@ -22,10 +22,13 @@
 
 namespace lcmc {
 
-__device__ __forceinline__ int grid_dim(double L, double wmin, int nc_max, int *flags)
+// Cells per axis: the largest count whose cells are at least wmin wide; an
+// even count (8-colour checkerboard) unless the replica takes the fine grid,
+// which keeps an odd count of 3 or more (3 colours on that axis).
+__device__ __forceinline__ int grid_dim(double L, double wmin, int nc_max, int fine, int *flags)
 {
     int m = (int)floor(L / wmin);
-    int nc = m >= 2 ? m - (m & 1) : 1;
+    int nc = m >= 2 ? ((fine && m >= 3) ? m : m - (m & 1)) : 1;
     if (nc > nc_max) {
         nc = nc_max;
         atomicOr(flags, F_GRIDCAP);
@@ -33,37 +36,47 @@ __device__ __forceinline__ int grid_dim(double L, double wmin, int nc_max, int *
     return nc;
 }
 
-// One block; thread r sets up replica r.  Then 8 threads scan the per-phase
-// active-cell counts over replicas.
+// One block; thread r sets up replica r.  Then a thread per colour phase
+// scans the phase's active-cell counts over replicas.
 __global__ void k_sweep_setup(DevView v)
 {
     for (int r = threadIdx.x; r < v.R; r += blockDim.x) {
         Replica &p = v.rep[r];
         for (int a = 0; a < 3; a++) {
-            p.nc[a] = grid_dim(p.L[a], p.wmin, p.nc_max, &v.stats[r].flags);
+            p.nc[a] = grid_dim(p.L[a], p.wmin, p.nc_max, p.fine, &v.stats[r].flags);
             p.w[a] = p.L[a] / (double)p.nc[a];
+            p.kc[a] = (p.nc[a] & 1) && p.nc[a] >= 3 ? 3 : 2;
         }
+        p.ncol = p.kc[0] * p.kc[1] * p.kc[2];
         U4 s = draw(p.key, SWEEP_ID, p.sweep, TAG_SHIFT);
         p.shift[0] = u01(s.x) * p.w[0];
         p.shift[1] = u01(s.y) * p.w[1];
         p.shift[2] = u01(s.z) * p.w[2];
+        // colour c = bx + kc0 (by + kc1 bz); with 8 colours c = bx + 2 by + 4 bz,
+        // drawn and shuffled exactly as before the fine grid existed
+        const int K = p.ncol;
+        uint32_t rr[LCMC_MAX_COLOURS + 1];
         U4 c0 = draw(p.key, SWEEP_ID, p.sweep, TAG_COLOUR);
         U4 c1 = draw(p.key, SWEEP_ID, p.sweep, TAG_COLOUR + 1);
-        uint32_t rr[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-        int perm[8];
-        for (int i = 0; i < 8; i++) perm[i] = i;
-        for (int i = 7; i >= 1; i--) { // Fisher-Yates (the reference shuffles its subcells, 646-648)
-            int j = (int)(rr[7 - i] % (uint32_t)(i + 1));
+        rr[0] = c0.x, rr[1] = c0.y, rr[2] = c0.z, rr[3] = c0.w, rr[4] = c1.x, rr[5] = c1.y, rr[6] = c1.z, rr[7] = c1.w;
+        for (int m = 0; 8 + 4 * m < K - 1; m++) {
+            const U4 e = draw(p.key, SWEEP_ID, p.sweep, TAG_COLOUR_EXT + (uint32_t)m);
+            rr[8 + 4 * m] = e.x, rr[9 + 4 * m] = e.y, rr[10 + 4 * m] = e.z, rr[11 + 4 * m] = e.w;
+        }
+        int perm[LCMC_MAX_COLOURS];
+        for (int i = 0; i < K; i++) perm[i] = i;
+        for (int i = K - 1; i >= 1; i--) { // Fisher-Yates (the reference shuffles its subcells, 646-648)
+            int j = (int)(rr[K - 1 - i] % (uint32_t)(i + 1));
             int t = perm[i];
             perm[i] = perm[j];
             perm[j] = t;
         }
-        for (int i = 0; i < 8; i++) p.perm[i] = perm[i];
+        for (int i = 0; i < LCMC_MAX_COLOURS; i++) p.perm[i] = i < K ? perm[i] : -1;
         p.use_fast = (p.kernel == 1) && p.nc[0] >= 4 && p.nc[1] >= 4 && p.nc[2] >= 4;
         p.vol_state = 0;
     }
     __syncthreads();
-    if (threadIdx.x < 8) {
+    if ((int)threadIdx.x < v.nphase) {
         int ci = threadIdx.x;
         v.resc_count[ci] = 0;
         int *off = v.act_off + ci * (v.R + 1);
@@ -71,12 +84,11 @@ __global__ void k_sweep_setup(DevView v)
         for (int r = 0; r < v.R; r++) {
             off[r] = acc;
             const Replica &p = v.rep[r];
-            int col = p.perm[ci];
+            const int col = p.perm[ci];
+            if (col < 0) continue; // this replica has fewer colours
+            const int b[3] = {col % p.kc[0], (col / p.kc[0]) % p.kc[1], col / (p.kc[0] * p.kc[1])};
             int cnt = 1;
-            for (int a = 0; a < 3; a++) {
-                int b = (col >> a) & 1;
-                cnt *= (p.nc[a] - b + 1) / 2;
-            }
+            for (int a = 0; a < 3; a++) cnt *= axis_colour_count(p.nc[a], p.kc[a], b[a]);
             acc += cnt;
         }
         off[v.R] = acc;

@@ -25,6 +25,7 @@ constexpr uint32_t TAG_SPHERE = 1u;    // 1..16: Marsaglia pairs, two per call
 constexpr uint32_t TAG_SHIFT = 0x100u; // per-sweep grid shift
 constexpr uint32_t TAG_COLOUR = 0x101u;// per-sweep colour order (two calls)
 constexpr uint32_t TAG_VOLUME = 0x103u;// per-sweep volume move
+constexpr uint32_t TAG_COLOUR_EXT = 0x110u; // 0x110..0x114: colour order beyond 8 colours (fine grid)
 constexpr uint32_t TAG_INIT = 0x200u;  // initial orientations (cone mode)
 constexpr uint32_t SWEEP_ID = 0xFFFFFFFFu;
 constexpr uint64_t INIT_SWEEP = 0xFFFFFFFFFFFFFFFFull;

@@ -53,14 +53,14 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
         const Replica &p = v.rep[r];
         if (p.use_fast) continue;
         const int col = p.perm[ci];
-        const int bx = col & 1, by = (col >> 1) & 1, bz = (col >> 2) & 1;
+        const int bx = col % p.kc[0], by = (col / p.kc[0]) % p.kc[1], bz = col / (p.kc[0] * p.kc[1]);
         const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
-        const int nax = (nc0 - bx + 1) / 2, nay = (nc1 - by + 1) / 2;
+        const int nax = axis_colour_count(nc0, p.kc[0], bx), nay = axis_colour_count(nc1, p.kc[1], by);
         int loc = a - off[r];
-        const int cx = 2 * (loc % nax) + bx;
+        const int cx = axis_colour_cell(nc0, p.kc[0], bx, loc % nax);
         loc /= nax;
-        const int cy = 2 * (loc % nay) + by;
-        const int cz = 2 * (loc / nay) + bz;
+        const int cy = axis_colour_cell(nc1, p.kc[1], by, loc % nay);
+        const int cz = axis_colour_cell(nc2, p.kc[2], bz, loc / nay);
         const int cell = p.cell_off + (cz * nc1 + cy) * nc0 + cx;
 
         // canonical stencil: dz, dy, dx = -1..1, duplicates dropped at first occurrence

@@ -144,13 +144,14 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
         const Replica &p = v.rep[r];
         if (!p.use_fast) continue; // uniform across the block
         const int col = p.perm[ci];
+        const int bx = col % p.kc[0], by = (col / p.kc[0]) % p.kc[1], bz = col / (p.kc[0] * p.kc[1]);
         const int nc0 = p.nc[0], nc1 = p.nc[1], nc2 = p.nc[2];
-        const int nax = nc0 >> 1, nay = nc1 >> 1;
+        const int nax = axis_colour_count(nc0, p.kc[0], bx), nay = axis_colour_count(nc1, p.kc[1], by);
         int loc = a - off[r];
-        const int cx = 2 * (loc % nax) + (col & 1);
+        const int cx = axis_colour_cell(nc0, p.kc[0], bx, loc % nax);
         loc /= nax;
-        const int cy = 2 * (loc % nay) + ((col >> 1) & 1);
-        const int cz = 2 * (loc / nay) + ((col >> 2) & 1);
+        const int cy = axis_colour_cell(nc1, p.kc[1], by, loc % nay);
+        const int cz = axis_colour_cell(nc2, p.kc[2], bz, loc / nay);
         const int cell = p.cell_off + (cz * nc1 + cy) * nc0 + cx;
         const double w0 = p.w[0], w1 = p.w[1], w2 = p.w[2];
         const FastK K = fast_consts(p.k);

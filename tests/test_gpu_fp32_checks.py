@@ -166,3 +166,70 @@ def test_npt_running_energy_tracks_the_recompute():
         assert st["drift_breaches"] == 0 and st["energy_checks"] == 30
         e = s.tot_ene()
         assert abs(st["energy"] - e) <= 1e-6 * (abs(e) + n)
+
+
+def _batch_params():
+    """Small boxes on the fine cell grid (odd counts allowed): 5, 6 and 7 cells
+    of about 4.7 per axis instead of 4, 6 and 6 cells up to 5.9 wide, so each
+    replica keeps the FP32 kernel; NVT, NPT and a colloid replica."""
+    common = dict(gb_kappa=3.0, gb_kappa_prime=5.0, gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
+                  max_displacement=0.1, max_rotation=0.1, precision_mode=1, cell_grid=1,
+                  init_orientation_cone_deg=20.0, init_lattice=1)
+    return [
+        lcmc.default_params(num_particles=4096, system_density=0.32, system_temperature=0.8, rng_seed=201, **common),
+        lcmc.default_params(num_particles=6000, system_density=0.32, system_temperature=1.2, rng_seed=202,
+                            mc_ensemble_type=2, system_pressure=2.0, **common),
+        lcmc.default_params(num_particles=8192, system_density=0.30, system_temperature=0.9, rng_seed=203,
+                            colloid_radius=3.0, colloid_wall_option=1, **common),
+    ]
+
+
+def test_fine_grid_batch_matches_single_runs_fp32():
+    """Replicas of a batch on the FP32 kernel (fine grid: up to 27 colour
+    phases) reproduce their single runs bit for bit."""
+    ps = _batch_params()
+    singles = []
+    for p in ps:
+        with lcmc.GBSystem(p) as s:
+            s.get_initial_config()
+            s.sweep(4)
+            st = s.stats()
+            assert st["kernel"] == 1, st
+            singles.append((s.download(), st))
+    with lcmc.GBSystem(ps) as b:
+        for r in range(len(ps)):
+            b.get_initial_config(r)
+        b.sweep(4)
+        for r, (want, wst) in enumerate(singles):
+            got = b.download(r)
+            for x, y in zip(got[0], want[0]):
+                assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
+            assert np.array_equal(got[1].view(np.uint64), want[1].view(np.uint64))
+            st = b.stats(r)
+            assert st["accepted"] == wst["accepted"] and st["energy"] == wst["energy"] and st["kernel"] == 1
+
+
+def test_fine_grid_fp32_decisions_match_fp64():
+    """Lockstep on a small box (N = 4096, 5 cells per axis, 3 colours on each
+    axis = 27 phases): FP32 against FP64 kernel decisions."""
+    p = _batch_params()[0]
+    st0, box = lcmc.lattice(p)
+    with lcmc.GBSystem(p) as a, lcmc.GBSystem(p) as b:
+        b.set_kernel(0)
+        b.upload(*st0, box)
+        b.sweep(20)
+        a.record_moves(True)
+        b.record_moves(True)
+        for _ in range(30):
+            x, bx = b.download()
+            a.upload(*x, bx)
+            _lib.check(_lib.lib().lcmc_set_sweep_counter(a._h, 0, b.stats()["sweeps"]))
+            a.sweep(1)
+            b.sweep(1)
+            oa, ob = a.outcomes(), b.outcomes()
+            ea, _ = a.move_records()
+            eb, _ = b.move_records()
+            soft = ob != 2
+            assert np.mean(oa[soft] == ob[soft]) >= 0.999
+            assert np.all(np.abs(ea - eb)[soft] <= 1e-3 + 1e-5 * np.abs(eb[soft]))
+        assert a.stats()["kernel"] == 1 and b.stats()["kernel"] == 0
