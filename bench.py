@@ -556,12 +556,32 @@ def batch_replica_params(lcmc, n_rep=64, seed=2024):
     return ps
 
 
-def batch_workload(lcmc, torch, steps, warmup, single_rate=None):
-    """Moves/s of the 64-replica batch in one graph-launched sweep (device time
-    per sweep, L2 flushed between sweeps), with the autotuner's choice."""
+def lpt_split(costs, world):
+    """Longest-processing-time placement of independent replicas on `world`
+    ranks: replicas in decreasing cost (ties: lower index first), each to the
+    rank with the least total cost so far (ties: lower rank).  Returns each
+    rank's replica indices in ascending order; every rank computes the same
+    split from the same costs, so no exchange is needed."""
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += costs[i]
+        parts[r].append(i)
+    return [sorted(p) for p in parts]
+
+
+def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank=0, world=1):
+    """Moves/s of the 64-replica batch in one graph-launched sweep per rank
+    (device time per sweep, L2 flushed between sweeps), with the autotuner's
+    choice.  With N ranks the replicas are split by longest-processing-time
+    on N x sweeps (every replica runs the same sweeps); the job's time is the
+    slowest rank's, and value counts every replica's moves."""
     import numpy as np
-    ps = batch_replica_params(lcmc)
-    ntot = sum(p.num_particles for p in ps)
+    ps_all = batch_replica_params(lcmc)
+    ntot = sum(p.num_particles for p in ps_all)
+    share = lpt_split([float(p.num_particles) for p in ps_all], world)[rank]
+    ps = [ps_all[i] for i in share]
     s = lcmc.GBSystem(ps)
     for r in range(len(ps)):
         s.get_initial_config(r)
@@ -571,6 +591,9 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     st0 = [s.stats(r) for r in range(len(ps))]
     ms, parts = [], []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
     for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -592,13 +615,16 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None):
     worst = max(abs(s.stats(r)["drift"]) / max(s.stats(r)["drift_bound"], 1e-300) for r in range(len(ps)))
     kps = s.kernels_per_sweep()
     s.close()
-    value = ntot * steps / (sum(ms) * 1e-3)
+    total_ms = max_over_ranks(dist, sum(ms))
+    value = ntot * steps / (total_ms * 1e-3)
     out = {"workload": "64 replicas, N log-uniform in [4096, 65536], T* U[0.6, 1.4], half NVT at rho* 0.30-0.34, "
                        "half NPT at P* 1.5-2.5, a third with a colloid R U[3, 6]; FP32 kernel, fine cell grid, "
                        "one CUDA graph per sweep over the replica table",
-           "replicas": len(ps), "n_total": ntot, "n_min": min(p.num_particles for p in ps),
-           "n_max": max(p.num_particles for p in ps), "steps": steps, "warmup": max(3, warmup),
-           "ms_per_step": statistics.mean(ms), "value": value, "unit": UNIT,
+           "replicas": len(ps_all), "n_total": ntot, "n_min": min(p.num_particles for p in ps_all),
+           "n_max": max(p.num_particles for p in ps_all), "steps": steps, "warmup": max(3, warmup),
+           "ms_per_step": total_ms / steps, "value": value, "unit": UNIT,
+           "placement": {"ranks": world, "rank0_replicas": len(ps),
+                         "rank0_particles": sum(p.num_particles for p in ps)},
            "replicas_on_fp32_kernel": int(sum(st["kernel"] for st in st1)),
            "fp64_cells_per_sweep": fp64_cells / steps,
            "ms_parts_median": {"rebin": parts[0], "colour_phases": parts[1], "stats_and_volume": parts[2],
@@ -761,8 +787,9 @@ def main():
     if args.jammed_steps > 0 and world == 1:
         jam = jammed_start(lcmc, torch, args.jammed_steps, args.warmup)
     batch = None
-    if args.batch_steps > 0 and world == 1:
-        batch = batch_workload(lcmc, torch, args.batch_steps, args.warmup, single_rate=value)
+    if args.batch_steps > 0:  # every rank takes part (its share of the replicas)
+        batch = batch_workload(lcmc, torch, args.batch_steps, args.warmup, single_rate=value, dist=dist, rank=rank,
+                               world=world)
 
     if rank != 0:
         if dist:

@@ -51,3 +51,52 @@ def test_single_process_is_unchanged():
     import bench
     assert bench.max_over_ranks(None, 3.25) == 3.25
     assert bench.job_rate(1048576, 1, 2.0) == 524288.0
+
+
+def _lpt_rank(rank, world, port, q):
+    sys.path.insert(0, REPO)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch.distributed as dist
+
+    import bench
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+
+    import numpy as np
+    rng = np.random.default_rng(2024)
+    sizes = [int(round(float(np.exp(rng.uniform(np.log(4096), np.log(65536)))))) for _ in range(64)]
+    mine = bench.lpt_split([float(n) for n in sizes], world)[rank]
+    views = [None] * world
+    dist.all_gather_object(views, mine)
+    q.put((rank, mine, views, sizes))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_lpt_split_over_two_gloo_ranks():
+    """Replica placement for bench.py --gpus N: each rank computes its share of
+    the 64-replica batch from the same sizes, with no exchange; the shares are
+    disjoint, cover every replica, and differ in total size by at most the
+    largest replica (the longest-processing-time bound)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_lpt_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, m0, v0, sizes), (_, m1, v1, _) = got
+    assert v0 == v1 == [m0, m1]
+    assert sorted(m0 + m1) == list(range(64))
+    loads = [sum(sizes[i] for i in m) for m in (m0, m1)]
+    assert abs(loads[0] - loads[1]) <= max(sizes)
+
+
+def test_lpt_split_single_rank_and_ties():
+    sys.path.insert(0, REPO)
+    import bench
+    assert bench.lpt_split([3.0, 1.0, 2.0], 1) == [[0, 1, 2]]
+    assert bench.lpt_split([5.0, 5.0, 5.0, 5.0], 2) == [[0, 2], [1, 3]]
+    assert bench.lpt_split([], 3) == [[], [], []]
