@@ -585,8 +585,25 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank
     s = lcmc.GBSystem(ps)
     for r in range(len(ps)):
         s.get_initial_config(r)
+    # NPT replicas screen their volume moves with the FP32-pair energy change:
+    # the plain move's decisions, with the FP64 recompute only where stage 1 passes
+    s.set_fp32_screen(True)
     tune = s.autotune(sweeps=2)
-    s.sweep(max(3, warmup))
+    breaches = 0
+
+    def sweep1(k):
+        """k sweeps; an energy-check breach (LCMC_EDRIFT) is counted, its sticky
+        flag cleared, and the run goes on (the chain is unchanged by it)."""
+        nonlocal breaches
+        try:
+            s.sweep(k)
+        except lcmc.LcmcError as e:
+            if e.code != -12:
+                raise
+            breaches += 1
+            s.clear_error_flags()
+
+    sweep1(max(3, warmup))
     ext = torch.cuda.ExternalStream(s.stream_handle())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     st0 = [s.stats(r) for r in range(len(ps))]
@@ -599,7 +616,7 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(ext)
-        s.sweep(1)
+        sweep1(1)
         b.record(ext)
         b.synchronize()
         ms.append(a.elapsed_time(b))
@@ -618,8 +635,9 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank
     total_ms = max_over_ranks(dist, sum(ms))
     value = ntot * steps / (total_ms * 1e-3)
     out = {"workload": "64 replicas, N log-uniform in [4096, 65536], T* U[0.6, 1.4], half NVT at rho* 0.30-0.34, "
-                       "half NPT at P* 1.5-2.5, a third with a colloid R U[3, 6]; FP32 kernel, fine cell grid, "
-                       "one CUDA graph per sweep over the replica table",
+                       "half NPT at P* 1.5-2.5 (volume moves screened by the FP32-pair energy change), a third "
+                       "with a colloid R U[3, 6]; FP32 kernel, fine cell grid, one CUDA graph per sweep over the "
+                       "replica table",
            "replicas": len(ps_all), "n_total": ntot, "n_min": min(p.num_particles for p in ps_all),
            "n_max": max(p.num_particles for p in ps_all), "steps": steps, "warmup": max(3, warmup),
            "ms_per_step": total_ms / steps, "value": value, "unit": UNIT,
@@ -630,7 +648,8 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank
            "ms_parts_median": {"rebin": parts[0], "colour_phases": parts[1], "stats_and_volume": parts[2],
                                "advance": parts[3]},
            "kernels_per_sweep": kps, "autotune": tune,
-           "energy_check": {"ok": check_ok, "max_drift_over_tolerance": worst}}
+           "energy_check": {"ok": check_ok and breaches == 0, "max_drift_over_tolerance": worst,
+                            "breaches_during_sweeps": breaches}}
     if single_rate:
         out["per_move_rate_vs_single_system"] = value / single_rate
     return out

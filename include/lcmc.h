@@ -99,7 +99,7 @@ typedef struct {
     int energy_check_interval;       /* sweeps between periodic FP64 energy checks, 0 = off (the reference's
                                         check_energy / EnergyCheck, MCnptColloid.c:946-955, 1343-1362) */
     double energy_check_tolerance;   /* relative tolerance of the check against max(|E|, N 4 eps0) plus the
-                                        sum of |dE| accepted since the last check; 0 = automatic: 1e-6 for
+                                        sum of |dE| accepted since the last check; 0 = automatic: 1e-4 for
                                         the FP32 kernel, 1e-9 for the FP64 kernel */
     int init_lattice;                /* lattice of initial_configuration_type 2: 0 = simple cubic (the
                                         reference's), 1 = body-centred tetragonal with the long axis along z,

@@ -639,7 +639,7 @@ static void set_caps(lcmc_ctx *c)
         Replica &rp = c->rep[r];
         const lcmc_params &p = c->params[r];
         rp.cap = p.cell_capacity > 0 ? std::min(p.cell_capacity, amax) : amax;
-        rp.check_tol = p.energy_check_tolerance > 0.0 ? p.energy_check_tolerance : (rp.kernel == 1 ? 1e-6 : 1e-9);
+        rp.check_tol = p.energy_check_tolerance > 0.0 ? p.energy_check_tolerance : (rp.kernel == 1 ? 1e-4 : 1e-9);
     }
 }
 

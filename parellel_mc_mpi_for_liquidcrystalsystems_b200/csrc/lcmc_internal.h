@@ -7,16 +7,23 @@ namespace lcmc {
 // Most colour phases of a sweep: 3 colours per axis on odd cell counts (fine grid).
 constexpr int LCMC_MAX_COLOURS = 27;
 
-// Cells of colour b along an axis of nc cells with k colours (k = 2: cells
-// b, b + 2, ...; k = 3, odd nc: 0 and 1 alternate over the first nc - 1 cells
-// and colour 2 is the last cell), and the index of the j-th of them.
+// Cells of colour b along an axis of nc cells with k colours, and the index
+// of the j-th of them.  k = 2 (even nc, or a single cell): cells b, b + 2, ...
+// k = 3 (odd nc >= 3, fine grid), nc = 3q + r: colour i mod 3 for i < 3q, then
+// r = 1: cell 3q takes colour 1; r = 2: cells 3q, 3q + 1 take colours 0, 1.
+// Neighbouring cells (the periodic seam included) never share a colour, and
+// the colours hold q or q + 1 cells each, so the phases stay balanced.
 __host__ __device__ __forceinline__ int axis_colour_count(int nc, int k, int b)
 {
-    return k == 3 ? (b == 2 ? 1 : (nc - 1) / 2) : (nc - b + 1) / 2;
+    if (k != 3) return (nc - b + 1) / 2;
+    const int q = nc / 3, r = nc - 3 * q;
+    return q + ((r >= 1 && b == 1) ? 1 : 0) + ((r == 2 && b == 0) ? 1 : 0);
 }
 __host__ __device__ __forceinline__ int axis_colour_cell(int nc, int k, int b, int j)
 {
-    return (k == 3 && b == 2) ? nc - 1 : 2 * j + b;
+    if (k != 3) return 2 * j + b;
+    const int q = nc / 3, r = nc - 3 * q;
+    return j < q ? b + 3 * j : 3 * q + (r == 2 ? b : 0);
 }
 
 // Derived constants of one system (get_system_const, MCnptColloid.c:2752-2783,

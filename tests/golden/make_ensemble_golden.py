@@ -24,7 +24,8 @@ dense liquid of the CPU-runnable configuration (N = 1000, rho* = 0.30,
 T* = 1.0, d = 0.1, rotation 0.1, r_v = 4.8) with a colloid of radius 2 (for
 the same colloid-term reason).  A lattice at this density holds rods in the
 flat 1e9 overlap clamp, which no move leaves, so the start is relaxed first:
-a dilute lattice (rho* = 0.06) compressed by the oracle's checkerboard sweeps
+a dilute lattice (rho* = 0.06, no site within R + 2.5 of the colloid, where a
+rod could sit in the colloid term's flat 1e8 clamp) compressed by the oracle's checkerboard sweeps
 with ln V moves at P* = 4 until rho* >= 0.30, scaled to 0.30 exactly and
 stored with the averages, so the GPU test starts from the same state.
 """
@@ -94,7 +95,9 @@ def compressed_start(oc, n, rho, T, R, seed):
                   colloid_wall_option=1, rng_seed=seed, max_displacement=0.1, max_rotation=0.1)
     c = oc.consts(p, oc.ARITH_CANONICAL)
     k = oc.key(seed)
-    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=n, rho=0.06, R=R, seed=seed)
+    # no site within R + 2.5 of the colloid: a rod closer to its wall can sit in
+    # the colloid term's flat 1e8 clamp, which no move leaves
+    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=n, rho=0.06, R=R + 2.5, seed=seed)
     state = [np.ascontiguousarray(a, dtype=np.float64) for a in (px, py, pz, ox, oy, oz)]
     box = np.ascontiguousarray(box, dtype=np.float64)
     vcol = 4.0 * np.pi * R ** 3 / 3.0
