@@ -571,7 +571,7 @@ def lpt_split(costs, world):
     return [sorted(p) for p in parts]
 
 
-def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank=0, world=1):
+def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank=0, world=1, relax=30):
     """Moves/s of the 64-replica batch in one graph-launched sweep per rank
     (device time per sweep, L2 flushed between sweeps), with the autotuner's
     choice.  With N ranks the replicas are split by longest-processing-time
@@ -588,7 +588,6 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank
     # NPT replicas screen their volume moves with the FP32-pair energy change:
     # the plain move's decisions, with the FP64 recompute only where stage 1 passes
     s.set_fp32_screen(True)
-    tune = s.autotune(sweeps=2)
     breaches = 0
 
     def sweep1(k):
@@ -603,6 +602,8 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank
             breaches += 1
             s.clear_error_flags()
 
+    sweep1(max(1, relax))  # untimed: the lattice starts relax their overlaps
+    tune = s.autotune(sweeps=2)
     sweep1(max(3, warmup))
     ext = torch.cuda.ExternalStream(s.stream_handle())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -640,6 +641,7 @@ def batch_workload(lcmc, torch, steps, warmup, single_rate=None, dist=None, rank
                        "replica table",
            "replicas": len(ps_all), "n_total": ntot, "n_min": min(p.num_particles for p in ps_all),
            "n_max": max(p.num_particles for p in ps_all), "steps": steps, "warmup": max(3, warmup),
+           "relax_sweeps": max(1, relax),
            "ms_per_step": total_ms / steps, "value": value, "unit": UNIT,
            "placement": {"ranks": world, "rank0_replicas": len(ps),
                          "rank0_particles": sum(p.num_particles for p in ps)},
@@ -695,6 +697,9 @@ def main():
     ap.add_argument("--npt-screen", action="store_true", help="npt workload with the FP32-pair volume screen")
     ap.add_argument("--jammed-steps", type=int, default=5,
                     help="timed sweeps of the simple-cubic (jammed) start sub-measurement (0 skips it)")
+    ap.add_argument("--relax-sweeps", type=int, default=30,
+                    help="untimed sweeps from the lattice start before the warm-up (the start relaxes its overlaps; "
+                         "the timed window is then sweeps relax+warmup+1 .. of the run)")
     ap.add_argument("--batch-steps", type=int, default=10,
                     help="timed sweeps of the 64-replica batch sub-measurement (0 skips it)")
     args = ap.parse_args()
@@ -742,6 +747,8 @@ def main():
     s = lcmc.GBSystem(params)
     s.get_initial_config()
     ext = torch.cuda.ExternalStream(s.stream_handle())
+    if args.relax_sweeps > 0:
+        s.sweep(args.relax_sweeps)
     for _ in range(max(3, args.warmup)):
         s.sweep(1)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -766,7 +773,7 @@ def main():
     if dist:
         dist.barrier()
     st1 = s.stats()
-    check = energy_check_record(lcmc, s, max(3, args.warmup) + args.steps)
+    check = energy_check_record(lcmc, s, args.relax_sweeps + max(3, args.warmup) + args.steps)
     attempted = st1["attempted"] - st0["attempted"]
     value = job_rate(N_PART * args.steps, world, total_ms * 1e-3)
 
@@ -808,7 +815,7 @@ def main():
     batch = None
     if args.batch_steps > 0:  # every rank takes part (its share of the replicas)
         batch = batch_workload(lcmc, torch, args.batch_steps, args.warmup, single_rate=value, dist=dist, rank=rank,
-                               world=world)
+                               world=world, relax=args.relax_sweeps)
 
     if rank != 0:
         if dist:
@@ -834,7 +841,10 @@ def main():
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded lattice, relaxing from the lattice start)",
         "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single system",
-                       l2="flushed between sweeps (256 MiB memset)"),
+                       l2="flushed between sweeps (256 MiB memset)",
+                       timed_window=f"sweeps {args.relax_sweeps + max(3, args.warmup) + 1}-"
+                                    f"{args.relax_sweeps + max(3, args.warmup) + args.steps} of the run from the "
+                                    "lattice start"),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * N_PART + 24 + 8,
                 "d2h_bytes_per_step": 6 * 8 * N_PART + 24 + 8,
                 "step": "lcmc_upload_with_energy (pinned host SoA, caller-carried energy) + lcmc_sweep + "

@@ -854,6 +854,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     c->grid_energy = energy_exact_blocks_per_sm() * c->sms;
     c->grid_screen = screen_blocks_per_sm() * c->sms;
     c->grid_fast = fast_blocks_per_sm(c->fast_variant) * c->sms;
+    rescue_init();
     int rc = upload_replica_table(c);
     if (rc) {
         free_ctx(c);

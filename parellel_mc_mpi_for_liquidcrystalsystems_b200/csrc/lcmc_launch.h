@@ -27,6 +27,7 @@ FastVariant fast_variant(int i);
 void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, int grid);
 // FP64 attempts of the cells the FP32 kernel handed over in colour phase ci
 void launch_phase_rescue(bool spec21, const DevView &v, cudaStream_t s, int ci, int grid);
+void rescue_init(); // once per process before the first hand-over launch
 int fast_blocks_per_sm(int variant);
 
 // lcmc_misc.cu

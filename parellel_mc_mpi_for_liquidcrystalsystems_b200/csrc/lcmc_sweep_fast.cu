@@ -748,14 +748,19 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(c
 // block over the candidates, then a fixed-order block sum.
 // dE = (E_new - E_old) + dU_colloid, accepted if dE <= 0 or ln u <= -beta dE
 // (MCnptColloid.c:2491-2574).  The FP32 state copy of an accepted particle is
-// written exactly as the FP32 kernel writes it.  No per-particle state in
-// shared memory, so any cell count works.  The other cells of the colour do
-// not interact with these, so running them after the FP32 kernel changes
-// nothing in the chain.
+// written exactly as the FP32 kernel writes it.  The stencil's FP64 states
+// are staged in shared memory once per cell (the own cell's entries updated
+// as moves are accepted) when they fit in RESCUE_CAP particles; a larger
+// stencil is read from global memory, so any cell count works.  The other
+// cells of the colour do not interact with these, so running them after the
+// FP32 kernel changes nothing in the chain.
+constexpr int RESCUE_CAP = 1024; // particles of a staged stencil (48 KB of shared memory)
+
 template <int NT, bool SPEC21>
 __global__ void __launch_bounds__(NT) k_phase_rescue(DevView v, int ci)
 {
     constexpr int NW = NT / 32;
+    extern __shared__ double sx[]; // [6][RESCUE_CAP]: x, y, z, ux, uy, uz of the staged stencil
     __shared__ int st_start[27], st_cnt[27], pre[28];
     __shared__ double spo[NW], spn[NW];
     __shared__ int snp[NW];
@@ -793,6 +798,25 @@ __global__ void __launch_bounds__(NT) k_phase_rescue(DevView v, int ci)
         __syncthreads();
         const int total = pre[27];
         const int g0 = st_start[13], na = st_cnt[13];
+        const bool staged = total <= RESCUE_CAP;
+        if (staged) {
+            for (int f = t; f < total; f += NT) {
+                int sl = 0, hi = 27;
+                while (hi - sl > 1) {
+                    const int mid = (sl + hi) >> 1;
+                    if (pre[mid] <= f) sl = mid;
+                    else hi = mid;
+                }
+                const int j = st_start[sl] + (f - pre[sl]);
+                sx[f] = v.px[j];
+                sx[RESCUE_CAP + f] = v.py[j];
+                sx[2 * RESCUE_CAP + f] = v.pz[j];
+                sx[3 * RESCUE_CAP + f] = v.ox[j];
+                sx[4 * RESCUE_CAP + f] = v.oy[j];
+                sx[5 * RESCUE_CAP + f] = v.oz[j];
+            }
+            __syncthreads();
+        }
         double dsum = 0.0, dabs = 0.0;
         int nacc = 0, nhard = 0;
         unsigned long long npairs = 0ull;
@@ -816,17 +840,24 @@ __global__ void __launch_bounds__(NT) k_phase_rescue(DevView v, int ci)
             const double en[3] = {v.tux[g], v.tuy[g], v.tuz[g]};
             double po = 0.0, pn = 0.0;
             int np = 0;
+            const int fk = pre[13] + k; // this particle's own entry
             for (int f = t; f < total; f += NT) {
-                int sl = 0, hi = 27;
-                while (hi - sl > 1) {
-                    const int mid = (sl + hi) >> 1;
-                    if (pre[mid] <= f) sl = mid;
-                    else hi = mid;
+                if (f == fk) continue;
+                double rj[3], ej[3];
+                if (staged) {
+                    rj[0] = sx[f], rj[1] = sx[RESCUE_CAP + f], rj[2] = sx[2 * RESCUE_CAP + f];
+                    ej[0] = sx[3 * RESCUE_CAP + f], ej[1] = sx[4 * RESCUE_CAP + f], ej[2] = sx[5 * RESCUE_CAP + f];
+                } else {
+                    int sl = 0, hi = 27;
+                    while (hi - sl > 1) {
+                        const int mid = (sl + hi) >> 1;
+                        if (pre[mid] <= f) sl = mid;
+                        else hi = mid;
+                    }
+                    const int j = st_start[sl] + (f - pre[sl]);
+                    rj[0] = v.px[j], rj[1] = v.py[j], rj[2] = v.pz[j];
+                    ej[0] = v.ox[j], ej[1] = v.oy[j], ej[2] = v.oz[j];
                 }
-                const int j = st_start[sl] + (f - pre[sl]);
-                if (j == g) continue;
-                const double rj[3] = {v.px[j], v.py[j], v.pz[j]};
-                const double ej[3] = {v.ox[j], v.oy[j], v.oz[j]};
                 double d[3];
                 double r2 = dist_fold(ro[0], ro[1], ro[2], rj[0], rj[1], rj[2], p.L, d);
                 if (r2 < p.k.rc2) {
@@ -869,6 +900,11 @@ __global__ void __launch_bounds__(NT) k_phase_rescue(DevView v, int ci)
                     v.ox[g] = en[0];
                     v.oy[g] = en[1];
                     v.oz[g] = en[2];
+                    if (staged) {
+                        const int fk = pre[13] + k;
+                        sx[fk] = rn[0], sx[RESCUE_CAP + fk] = rn[1], sx[2 * RESCUE_CAP + fk] = rn[2];
+                        sx[3 * RESCUE_CAP + fk] = en[0], sx[4 * RESCUE_CAP + fk] = en[1], sx[5 * RESCUE_CAP + fk] = en[2];
+                    }
                     const float4 c4 = v.cl4[g];
                     float tux, tuy, tuz;
                     unit_f32(en[0], en[1], en[2], tux, tuy, tuz);
@@ -951,8 +987,17 @@ void launch_phase_fast(int variant, const DevView &v, cudaStream_t s, int ci, in
 
 void launch_phase_rescue(bool spec21, const DevView &v, cudaStream_t s, int ci, int grid)
 {
-    if (spec21) k_phase_rescue<256, true><<<grid, 256, 0, s>>>(v, ci);
-    else k_phase_rescue<256, false><<<grid, 256, 0, s>>>(v, ci);
+    const int bytes = 6 * RESCUE_CAP * (int)sizeof(double);
+    if (spec21) k_phase_rescue<256, true><<<grid, 256, bytes, s>>>(v, ci);
+    else k_phase_rescue<256, false><<<grid, 256, bytes, s>>>(v, ci);
+}
+
+// Opts the hand-over kernel in to its dynamic shared memory (call once).
+void rescue_init()
+{
+    const int bytes = 6 * RESCUE_CAP * (int)sizeof(double);
+    cudaFuncSetAttribute(k_phase_rescue<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_phase_rescue<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 // Also opts the variant in to its dynamic shared memory size: call once

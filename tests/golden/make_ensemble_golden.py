@@ -19,6 +19,12 @@ lattice within the burn-in (with d = 0.1 the energy still drifted by 6 % over
 10^4 sweeps).  The script prints the means of the two halves of the
 production run as a stationarity check.
 
+`make_ensemble_golden.py part K` runs the gas chain with seed SEED + K into
+ensemble_part_K.npz (independent chains can run on separate cores), and
+`make_ensemble_golden.py combine K1 K2 ...` merges those parts with the main
+chain into ensemble_golden.npz: the mean over every chain's blocks, with the
+standard error of all blocks taken together.
+
 `make_ensemble_golden.py dense` writes ensemble_dense_golden.npz instead: the
 dense liquid of the CPU-runnable configuration (N = 1000, rho* = 0.30,
 T* = 1.0, d = 0.1, rotation 0.1, r_v = 4.8) with a colloid of radius 2 (for
@@ -120,10 +126,36 @@ def compressed_start(oc, n, rho, T, R, seed):
     return state, box
 
 
+def combine(parts):
+    """The main chain (ensemble_golden.npz, its u/p2 series every 10 sweeps
+    and its block means) plus independent chains ensemble_part_K.npz: every
+    chain cut into BLOCKS blocks; the golden mean is the mean of all blocks and
+    its standard error the blocks' spread over the square root of their count."""
+    main_f = os.path.join(HERE, "ensemble_golden.npz")
+    files = [main_f] + [os.path.join(HERE, f"ensemble_part_{k}.npz") for k in parts]
+    bu, bp = [], []
+    for f in files:
+        g = np.load(f)
+        for v, dst in ((g["u_series"], bu), (g["p2_series"], bp)):
+            dst.extend(x.mean() for x in np.array_split(np.asarray(v), int(g["blocks"])))
+    g = dict(np.load(main_f))
+    g["u_mean"], g["u_se"] = float(np.mean(bu)), float(np.std(bu, ddof=1) / np.sqrt(len(bu)))
+    g["p2_mean"], g["p2_se"] = float(np.mean(bp)), float(np.std(bp, ddof=1) / np.sqrt(len(bp)))
+    g["chains"] = len(files)
+    np.savez(main_f, **g)
+    print(f"{len(files)} chains: U/N = {g['u_mean']:.6f} +- {g['u_se']:.6f}  P2 = {g['p2_mean']:.6f} +- "
+          f"{g['p2_se']:.6f} -> {main_f}")
+
+
 def main():
     import oracle_ctypes as oc
     global N, RHO, T, R_COLL, SEED, DMAX, ROT, BURN, SWEEPS, PARAM_TEXT
+    if len(sys.argv) > 1 and sys.argv[1] == "combine":
+        return combine([int(k) for k in sys.argv[2:]])
     dense = len(sys.argv) > 1 and sys.argv[1] == "dense"
+    part = int(sys.argv[2]) if len(sys.argv) > 2 and sys.argv[1] == "part" else None
+    if part is not None:
+        SEED = SEED + part
     if dense:
         N, RHO, T, R_COLL, SEED, DMAX, ROT, BURN, SWEEPS = 1000, 0.30, 1.0, 2.0, 4343, 0.1, 0.1, 2000, 10000
         PARAM_TEXT = (PARAM_TEXT.replace("num_particles 1728", f"num_particles {N}")
@@ -174,6 +206,8 @@ def main():
     h = SWEEPS // 2
     print(f"halves: U/N {u[:h].mean():.5f} {u[h:].mean():.5f}  P2 {p2[:h].mean():.5f} {p2[h:].mean():.5f}")
     out = os.path.join(HERE, "ensemble_dense_golden.npz" if dense else "ensemble_golden.npz")
+    if part is not None:
+        out = os.path.join(HERE, f"ensemble_part_{part}.npz")
     extra = {}
     if dense:
         extra = dict(start_px=start[0], start_py=start[1], start_pz=start[2], start_ox=start[3], start_oy=start[4],
