@@ -75,7 +75,7 @@ def test_dense_liquid_matches_reference_chain(golden):
     with lcmc.GBSystem(ps) as s:
         for r in range(REPLICAS):
             s.upload(*start, box, replica=r)
-        s.sweep(500)
+        s.sweep(int(g["burn"]))  # the reference chain's burn-in from the same start
         s.record_history(2500)
         s.sweep(2500)
         u = np.array([da.p2_series(s, r)[2].mean() / n for r in range(REPLICAS)])
