@@ -744,7 +744,8 @@ static double butterfly32(double part[32])
 /* One checkerboard sweep: per sweep a random grid shift and shuffled colour
  * order; per colour every active cell; per active cell its particles in
  * ascending id, each attempted once with the per-move semantics of
- * attempt_monte_carlo_move (MCnptColloid.c:2474-2598):
+ * attempt_monte_carlo_move (MCnptColloid.c:2474-2598), a move out of the
+ * particle's cell rejected (leaves_cell):
  *   E_old = sum_j phi(old, j) + U_coll(old)          (2491-2498)
  *   trial r' = r + d (u - 1/2) per axis, wrapped       (2502-2512)
  *   colloid hard-core reject if |r' - C|^2 <= R^2     (2516-2520)
@@ -754,26 +755,51 @@ static double butterfly32(double part[32])
  * with the colloid term added only when colloid_wall_option == 1 and Philox
  * draws in place of rand().  The sums over the stencil use the canonical
  * 32-way order of butterfly32. */
-/* One trial move of particle k against the staged stencil particles slots[0..S)
- * (attempt_monte_carlo_move, MCnptColloid.c:2474-2598, with the checkerboard's
- * pick and Philox draws): 0 rejected, 1 accepted (state written, *de set),
- * 2 hard-core reject. */
+/* Checkerboard rule for detailed balance: a trial translation that carries the
+ * particle out of the cell (cx, cy, cz) it was binned into at the sweep's start
+ * is rejected without an energy evaluation, so that the cells' contents and the
+ * order of the attempts stay fixed during the sweep (the rule of parallel
+ * hard-particle MC on GPUs, Anderson et al., J. Comput. Phys. 254 (2013) 27;
+ * the reference's random-sequential pick needs none).  Same operations, in the
+ * same order, as the GPU kernels' leaves_cell. */
+static int leaves_cell(const lco_grid *g, const int cell[3], const double ro[3], const double dsp[3],
+                       const double box[3])
+{
+    for (int a = 0; a < 3; a++) {
+        double o = g->shift[a] + (double)cell[a] * g->w[a];
+        double r = ro[a] - o;
+        double k = rint((r - 0.5 * g->w[a]) * (1.0 / box[a]));
+        double rel = r - box[a] * k;
+        double nr = rel + dsp[a];
+        if (!(nr >= 0.0 && nr < g->w[a])) return 1;
+    }
+    return 0;
+}
+
+/* One trial move of particle k of cell `cell` against the staged stencil
+ * particles slots[0..S) (attempt_monte_carlo_move, MCnptColloid.c:2474-2598,
+ * with the checkerboard's pick and Philox draws): 0 rejected (also a move out
+ * of the cell), 1 accepted (state written, *de set), 2 hard-core reject. */
 static int attempt_move(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int k, const int *slots, int S,
                         double *px, double *py, double *pz, double *ox, double *oy, double *oz, const double box[3],
-                        double *de_out)
+                        const lco_grid *g, const int cell[3], double *de_out)
 {
     uint32_t rnd[4];
     philox_at(key, (uint32_t)k, sweep, TAG_MOVE, rnd);
     double ro[3] = {px[k], py[k], pz[k]}, eo[3] = {ox[k], oy[k], oz[k]};
-    double rn[3];
-    rn[0] = ro[0] + c->max_disp * (lco_u01(rnd[0]) - 0.5);
-    rn[1] = ro[1] + c->max_disp * (lco_u01(rnd[1]) - 0.5);
-    rn[2] = ro[2] + c->max_disp * (lco_u01(rnd[2]) - 0.5);
+    double rn[3], dsp[3];
+    dsp[0] = c->max_disp * (lco_u01(rnd[0]) - 0.5);
+    dsp[1] = c->max_disp * (lco_u01(rnd[1]) - 0.5);
+    dsp[2] = c->max_disp * (lco_u01(rnd[2]) - 0.5);
+    rn[0] = ro[0] + dsp[0];
+    rn[1] = ro[1] + dsp[1];
+    rn[2] = ro[2] + dsp[2];
     lco_apply_pbc(&rn[0], &rn[1], &rn[2], box);
     double ddx, ddy, ddz;
     double rc2c = lco_distance_sq(rn[0], rn[1], rn[2], 0.5 * box[0], 0.5 * box[1], 0.5 * box[2], box, &ddx, &ddy,
                                   &ddz);
     if (!(rc2c > c->coll_R * c->coll_R)) return 2;
+    if (leaves_cell(g, cell, ro, dsp, box)) return 0;
     double v[3];
     lco_sphere_point(key, (uint32_t)k, sweep, v);
     double en[3];
@@ -848,13 +874,14 @@ int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n,
             for (int cy = by; cy < g.nc[1]; cy += 2)
                 for (int cx = bx; cx < g.nc[0]; cx += 2) {
                     int cell = (cz * g.nc[1] + cy) * g.nc[0] + cx;
+                    const int cc[3] = {cx, cy, cz};
                     int S = stage_stencil(&g, cx, cy, cz, slots);
                     for (int a = g.cell_start[cell]; a < g.cell_start[cell + 1]; a++) {
                         int k = g.order[a];
                         if (order_out) order_out[st->attempted] = k;
                         st->attempted++;
                         double de = 0.0;
-                        int r = attempt_move(c, key, sweep, k, slots, S, px, py, pz, ox, oy, oz, box, &de);
+                        int r = attempt_move(c, key, sweep, k, slots, S, px, py, pz, ox, oy, oz, box, &g, cc, &de);
                         if (accept_bits) accept_bits[nb] = (unsigned char)r;
                         nb++;
                         if (r == 2) st->hardcore_rejected++;
@@ -899,10 +926,12 @@ int lco_sweep_parallel(const lco_consts *c, const uint32_t key[2], uint64_t swee
             for (long e = 0; e < ncell; e++) {
                 int cx = bx + 2 * (int)(e % hx), cy = by + 2 * (int)((e / hx) % hy), cz = bz + 2 * (int)(e / ((long)hx * hy));
                 int cell = (cz * g.nc[1] + cy) * g.nc[0] + cx;
+                const int cc[3] = {cx, cy, cz};
                 int S = stage_stencil(&g, cx, cy, cz, slots);
                 for (int a = g.cell_start[cell]; a < g.cell_start[cell + 1]; a++) {
                     double de = 0.0;
-                    int r = attempt_move(c, key, sweep, g.order[a], slots, S, px, py, pz, ox, oy, oz, box, &de);
+                    int r = attempt_move(c, key, sweep, g.order[a], slots, S, px, py, pz, ox, oy, oz, box, &g, cc,
+                                         &de);
                     att++;
                     if (r == 2) hard++;
                     if (r == 1) {

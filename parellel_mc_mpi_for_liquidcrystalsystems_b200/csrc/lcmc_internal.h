@@ -151,7 +151,7 @@ struct DevView {
     double *tdU;               // colloid-term change
     double *tlu;               // log of the Metropolis draw
     float *tdx, *tdy, *tdz;    // displacement
-    unsigned char *thard;      // 1 = colloid hard-core reject
+    unsigned char *thard;      // 0 evaluate, 1 colloid hard-core reject, 3 leaves its cell (rejected)
     // FP32 copy of the state of FP32-kernel systems, relative to each particle's
     // own cell origin: (x, y, z, ux) and (uy, uz), unit orientation; written by
     // the gather, kept current by the phase write-back

@@ -254,8 +254,12 @@ __global__ void k_gather(DevView v)
         if (!p.use_fast) continue;
         double rn[3], en[3], dsp[3], u;
         const int ok = make_trial(p, (uint32_t)id, ro, eo, rn, en, dsp, &u);
+        const int cl = v.cid[src] - p.cell_off;
+        const int cx = cl % p.nc[0], cy = (cl / p.nc[0]) % p.nc[1], cz = cl / (p.nc[0] * p.nc[1]);
+        // 0 trial to evaluate, 1 colloid hard-core reject, 3 leaves its cell (rejected)
+        const unsigned char code = !ok ? 1 : (leaves_cell(p, cx, cy, cz, ro, dsp) ? 3 : 0);
         double dU = 0.0;
-        if (ok && p.k.coll_on) dU = colloid_rod(p.k, rn, en, p.L) - colloid_rod(p.k, ro, eo, p.L);
+        if (code == 0 && p.k.coll_on) dU = colloid_rod(p.k, rn, en, p.L) - colloid_rod(p.k, ro, eo, p.L);
         v.tnx[g] = rn[0];
         v.tny[g] = rn[1];
         v.tnz[g] = rn[2];
@@ -267,10 +271,8 @@ __global__ void k_gather(DevView v)
         v.tdz[g] = (float)dsp[2];
         v.tdU[g] = dU;
         v.tlu[g] = log_unit(u);
-        v.thard[g] = (unsigned char)!ok;
+        v.thard[g] = code;
         // FP32 copy relative to the particle's own cell origin
-        const int cl = v.cid[src] - p.cell_off;
-        const int cx = cl % p.nc[0], cy = (cl / p.nc[0]) % p.nc[1], cz = cl / (p.nc[0] * p.nc[1]);
         const double lx = fold_rel(ro[0], p.shift[0] + (double)cx * p.w[0], 0.5 * p.w[0], p.L[0], 1.0 / p.L[0]);
         const double ly = fold_rel(ro[1], p.shift[1] + (double)cy * p.w[1], 0.5 * p.w[1], p.L[1], 1.0 / p.L[1]);
         const double lz = fold_rel(ro[2], p.shift[2] + (double)cz * p.w[2], 0.5 * p.w[2], p.L[2], 1.0 / p.L[2]);

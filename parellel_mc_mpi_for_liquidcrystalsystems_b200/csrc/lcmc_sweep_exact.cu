@@ -101,6 +101,16 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
             double eo[3] = {v.ox[g], v.oy[g], v.oz[g]};
             double rn[3], en[3], dsp[3], uacc;
             int ok = make_trial(p, id, ro, eo, rn, en, dsp, &uacc);
+            if (ok && leaves_cell(p, cx, cy, cz, ro, dsp)) { // out of its cell: rejected, no energy evaluation
+                if (lane == 0) {
+                    v.outcome[p.p_off + id] = 0;
+                    if (v.rec_dE) {
+                        v.rec_dE[p.p_off + id] = 0.0;
+                        v.rec_lu[p.p_off + id] = log_unit(uacc);
+                    }
+                }
+                continue;
+            }
             if (!ok) {
                 if (lane == 0) {
                     v.outcome[p.p_off + id] = 2;

@@ -701,7 +701,10 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(c
                 dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
                 dabs += __shfl_xor_sync(0xffffffffu, dabs, o);
             }
-            const int nacc = __popc(acc0) + __popc(acc1), nhard = __popc(hd0) + __popc(hd1);
+            // colloid hard-core rejects (code 1) counted apart from moves that leave their cell (code 3)
+            const unsigned hc0 = __ballot_sync(0xffffffffu, v0 && sm.hard[lane] == 1);
+            const unsigned hc1 = __ballot_sync(0xffffffffu, v1 && sm.hard[lane + 32] == 1);
+            const int nacc = __popc(acc0) + __popc(acc1), nhard = __popc(hc0) + __popc(hc1);
             if (lane == 0) {
                 if (!(dsum - dsum == 0.0)) atomicOr(&v.stats[r].flags, F_NONFINITE);
                 v.cell_e0[cell] = dsum;
@@ -730,7 +733,7 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(c
                 v.cl4[g] = make_float4(P1.z, P1.w, P2.x, P2.y);
                 v.cl2[g] = make_float2(P2.z, P2.w);
             }
-            v.outcome[p.p_off + sm.pid[k]] = sm.hard[k] ? 2 : acc;
+            v.outcome[p.p_off + sm.pid[k]] = sm.hard[k] == 1 ? 2 : acc;
         }
         __syncthreads();
     }
@@ -823,15 +826,16 @@ __global__ void __launch_bounds__(NT) k_phase_rescue(DevView v, int ci)
         for (int k = 0; k < na; k++) {
             const int g = g0 + k;
             const int id = v.id[g];
-            if (v.thard[g]) { // colloid hard-core reject: no energy evaluation
+            const unsigned char code = v.thard[g];
+            if (code) { // colloid hard-core reject (1) or a move out of the cell (3): no energy evaluation
                 if (t == 0) {
-                    v.outcome[p.p_off + id] = 2;
+                    v.outcome[p.p_off + id] = code == 1 ? 2 : 0;
                     if (v.rec_dE) {
                         v.rec_dE[p.p_off + id] = 0.0;
                         v.rec_lu[p.p_off + id] = v.tlu[g];
                     }
                 }
-                nhard++;
+                nhard += code == 1;
                 continue;
             }
             const double ro[3] = {v.px[g], v.py[g], v.pz[g]};

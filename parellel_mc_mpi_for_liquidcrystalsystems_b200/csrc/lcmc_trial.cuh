@@ -18,6 +18,35 @@ __device__ __forceinline__ double fold_rel(double x, double o, double cexp, doub
     return r - L * rint((r - cexp) * invL);
 }
 
+// Checkerboard rule for detailed balance: a trial translation that carries a
+// particle out of the cell it was binned into at the start of the sweep is
+// rejected without an energy evaluation.  Within a sweep the cell of every
+// particle then stays fixed, so the cells' contents and the order of the
+// attempts do not depend on the moves made (a move that crossed a cell face
+// would change both, and the sweep would no longer leave the Boltzmann
+// distribution invariant); the random grid shift of every sweep keeps the
+// chain ergodic.  The same rule as parallel hard-particle MC on GPUs
+// (Anderson et al., J. Comput. Phys. 254 (2013) 27).  The reference's
+// random-sequential schedule (MCnptColloid.c:2474-2598) needs no such rule.
+// (cx, cy, cz): the cell; ro: the position at the sweep's start; dsp: the
+// unwrapped displacement.  Rounded operations throughout, so every kernel and
+// the CPU oracle decide alike.
+__device__ __forceinline__ bool leaves_cell(const Replica &p, int cx, int cy, int cz, const double ro[3],
+                                            const double dsp[3])
+{
+    const int c[3] = {cx, cy, cz};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double o = __dadd_rn(p.shift[a], __dmul_rn((double)c[a], p.w[a]));
+        const double r = __dsub_rn(ro[a], o);
+        const double k = rint(__dmul_rn(__dsub_rn(r, __dmul_rn(0.5, p.w[a])), __ddiv_rn(1.0, p.L[a])));
+        const double rel = __dsub_rn(r, __dmul_rn(p.L[a], k));
+        const double nr = __dadd_rn(rel, dsp[a]);
+        if (!(nr >= 0.0 && nr < p.w[a])) return true;
+    }
+    return false;
+}
+
 // FP32 unit orientation of an FP64 orientation, with explicitly rounded FP64
 // operations (no contraction into FMA, whatever the file's flags), so every
 // kernel that forms it gets the same bits: the FP32 state copy written by the
