@@ -106,6 +106,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.first = 0
 
     def __enter__(self):
         try:
@@ -114,6 +115,11 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the sampler's first line marks it running; later lines fall in the timed region
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.first = len(self.lines)
         except Exception:
             self.proc = None
         return self
@@ -133,7 +139,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        lines = self.lines[self.first:] or self.lines
+        for l in lines:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
@@ -153,12 +160,14 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU reference (oracle/_ref/libmcref_omp.so: the reference's own functions)
 # ---------------------------------------------------------------------------
-def reference_cpu(n_part, seconds=12.0, threads=None):
-    """Time the reference's attempt_monte_carlo_move on the workload for about
-    `seconds` (a bounded sample).  The Verlet list (r_v = 4.8) is built once
-    with the same content as the reference's build_neighbor_lists (its O(N^2)
-    double loop is infeasible at N = 1M) and not rebuilt inside the sample,
-    which favours the reference."""
+def reference_cpu(n_part, seconds=12.0, threads=None, steps=1, warmup=0):
+    """Time the reference's attempt_monte_carlo_move on the workload: `warmup`
+    untimed and `steps` timed steps, each a bounded sample of the same number
+    of consecutive attempts, sized so that the timed steps take about
+    `seconds` together.  The Verlet list (r_v = 4.8) is built once with the
+    same content as the reference's build_neighbor_lists (its O(N^2) double
+    loop is infeasible at N = 1M) and not rebuilt inside the sample, which
+    favours the reference."""
     sys.path.insert(0, os.path.join(REPO, "tests"))
     import numpy as np
 
@@ -204,17 +213,26 @@ def reference_cpu(n_part, seconds=12.0, threads=None):
     t_list = time.perf_counter() - t0
     E = D(0.0)
     acc, nreb = C.c_long(0), C.c_long(0)
-    # calibrate, then a sample of about `seconds`
+    def run(k):
+        return ref.refdrv_run_attempts(k, 0, *ptrs, cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap,
+                                       C.byref(E), C.byref(acc), C.byref(nreb))
+
+    # calibrate, then `warmup` + `steps` steps of n_step attempts each
     n_try = 20
-    dt = ref.refdrv_run_attempts(n_try, 0, *ptrs, cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap, C.byref(E),
-                                 C.byref(acc), C.byref(nreb))
-    n_att = max(50, int(n_try * seconds / max(dt, 1e-6)))
-    dt = ref.refdrv_run_attempts(n_att, 0, *ptrs, cnt.ctypes.data_as(IP), lst.ctypes.data_as(IP), cap, C.byref(E),
-                                 C.byref(acc), C.byref(nreb))
+    dt = run(n_try)
+    steps = max(1, steps)
+    n_step = max(10, int(n_try * seconds / steps / max(dt, 1e-6)))
+    for _ in range(warmup):
+        run(n_step)
+    step_s = [run(n_step) for _ in range(steps)]
+    dt = sum(step_s)
+    n_att = n_step * steps
     return {"value": n_att / dt, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"{n_att} attempt_monte_carlo_move calls (MCnptColloid.c:2445) at N={n_part} in {dt:.1f} s, "
-                      f"OpenMP threads={threads}, Verlet list (r_v=4.8) built once in {t_list:.1f} s and not rebuilt",
-            "seconds": dt}, None
+            "sample": f"{steps} timed steps of {n_step} consecutive attempt_monte_carlo_move calls "
+                      f"(MCnptColloid.c:2445) at N={n_part}, {n_att} attempts in {dt:.1f} s after {warmup} untimed "
+                      f"steps, OpenMP threads={threads}, Verlet list (r_v=4.8) built once in {t_list:.1f} s and "
+                      "not rebuilt",
+            "seconds": dt, "attempts_per_step": n_step, "ms_per_step": 1e3 * dt / steps}, None
 
 
 # ---------------------------------------------------------------------------
@@ -250,10 +268,12 @@ def measured_peaks():
 
 def kernel_traffic():
     """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
-    k_phase_fast launch on this workload, from an ncu --set full capture of
-    launches 17-18 of `bench.py --steps 3 --warmup 3 --e2e-steps 1
-    --cpu-seconds 2 --da-sweeps 0` (44.0 MB read + 0.95 MB written)."""
-    return 44.0064e6 + 0.949504e6
+    k_phase_fast launch on this workload and where the figure comes from: a
+    fixed ncu capture (ncu cannot run inside the timed process), so it is
+    the same in every run and is refreshed when the kernel changes."""
+    return 44.0064e6 + 0.949504e6, ("fixed, from one ncu --set full capture of k_phase_fast launches 17-18 of "
+                                    "`bench.py --steps 3 --warmup 3 --e2e-steps 1 --cpu-seconds 2 --da-sweeps 0` "
+                                    "(44.0 MB read + 0.95 MB written per launch); not measured in this run")
 
 
 # ---------------------------------------------------------------------------
@@ -681,7 +701,7 @@ def job_rate(units_per_rank, world, seconds):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
@@ -710,16 +730,18 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        res, why = reference_cpu(N_PART, seconds=max(2.0, args.cpu_seconds))
+        steps = max(1, args.steps)
+        res, why = reference_cpu(N_PART, seconds=max(2.0, args.cpu_seconds), steps=steps, warmup=args.warmup)
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return 0
-        steps = max(1, args.steps)
         line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
-                "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * N_PART / res["value"],
+                "steps": steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded lattice)",
-                "config": dict(WORKLOAD, parallelism="cpu openmp", precision="fp64 (the reference's own code)"),
+                "data": "synthetic (seeded body-centred lattice, the GPU arm's start)",
+                "config": dict(WORKLOAD, parallelism="cpu openmp", precision="fp64 (the reference's own code)",
+                               step=f"a bounded sample of {res['attempts_per_step']} consecutive attempts of the "
+                                    f"N={N_PART} system (a sweep is {N_PART} attempts)"),
                 "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -854,7 +876,7 @@ def main():
                      "unit": "TFLOP/s", "frac": achieved / sgemm,
                      "peak_source": "cuBLAS FP32 SGEMM (TF32 off) measured in this run; nominal FP32 "
                                     f"{nominal:.1f} TFLOP/s at max clock",
-                     "traffic": traffic, "flop_per_attempt": flop_att, "stencil_candidates_per_attempt": C_att,
+                     "traffic": traffic[0], "traffic_source": traffic[1], "flop_per_attempt": flop_att, "stencil_candidates_per_attempt": C_att,
                      "in_cutoff_pairs_per_attempt_old_plus_new": P2_att, "avg_launch_ms": avg_launch_ms,
                      "phase_share_of_step": statistics.mean(phase_ms) / (total_ms / args.steps)},
         "cpu_baseline": cpu if cpu else {"unavailable": why},

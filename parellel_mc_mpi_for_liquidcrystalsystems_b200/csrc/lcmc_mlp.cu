@@ -25,82 +25,144 @@ using bf16 = __nv_bfloat16;
 // ---------------------------------------------------------------------------
 // C[M x N] (FP32, row-major) (+)= A[M x K] * B[N x K]^T; A, B BF16 row-major
 // with K contiguous (lda, ldb in elements, multiples of 8), K a multiple of 64.
-// CTA = 128 threads per 128 x 128 output tile.  Each 64-wide K slice of A and
-// B is staged in shared memory in the K-major core-matrix layout (8 rows x 16
-// bytes per core matrix, K halves 128 B apart, 8-row groups 1024 B apart); one
-// elected thread issues four 128x128x16 MMAs and commits them to an mbarrier;
-// the accumulator lives in 128 TMEM columns and is read back with tcgen05.ld
-// (warp w owns TMEM lanes 32w..32w+31 = rows).  Waits are bounded: on a
-// timeout the tile sets *err and frees its TMEM.
+// CTA = 128 threads per 128 x BN output tile (BN = 128, or 64 when 128-wide
+// tiles would leave most SMs idle).  The K loop runs over 64-wide slices
+// through a GT_STAGES-deep ring of shared-memory stages filled by cp.async
+// (16-byte copies, zero-filled beyond M and N) in the K-major core-matrix
+// layout (8 rows x 16 bytes per core matrix, K halves 128 B apart, 8-row
+// groups 1024 B apart).  One elected thread issues the slice's four
+// 128 x BN x 16 tcgen05 MMAs and commits them to the stage's mbarrier; a stage
+// is refilled once the MMAs that read it have completed, so GT_STAGES - 1
+// slices of loads are in flight while the tensor core works.  The accumulator
+// lives in BN TMEM columns and is read back with tcgen05.ld (warp w owns TMEM
+// lanes 32w..32w+31 = rows).  Waits are bounded: on a timeout the tile sets
+// *err, lets its copies and MMAs in flight finish and frees its TMEM.
 // ---------------------------------------------------------------------------
-constexpr int GT_M = 128, GT_N = 128, GT_K = 64;
+constexpr int GT_M = 128, GT_K = 64, GT_STAGES = 4;
 // mbarrier tries before a wait gives up (lcmc_set_wait_limit lowers it for tests)
 constexpr uint32_t kWaitIters = 1u << 24;
 static uint32_t g_wait_iters = kWaitIters;
 
+template <int BN> struct GemmShape {
+    static constexpr int A_BYTES = GT_M * GT_K * 2, B_BYTES = BN * GT_K * 2, STAGE = A_BYTES + B_BYTES;
+    static constexpr int SMEM = GT_STAGES * STAGE;
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(tc::smem_u32(smem)), "l"(gmem),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Slice kt of A (128 rows from m0) and B (BN rows from n0) into one stage (sA, sB).
+template <int BN>
+__device__ __forceinline__ void gemm_load_slice(unsigned char *sA, unsigned char *sB, const bf16 *__restrict__ A,
+                                                int lda, const bf16 *__restrict__ B, int ldb, int M, int N, int m0,
+                                                int n0, int kt, int t)
+{
+    const int k0 = kt * GT_K;
+#pragma unroll
+    for (int i = 0; i < GT_M * 8 / 128; i++) {
+        const int v = t + 128 * i;
+        const int row = v >> 3, ch = v & 7;
+        const int off = ((row >> 3) * 8 + ch) * 128 + (row & 7) * 16;
+        const int gm = m0 + row;
+        const bool in = gm < M;
+        cp_async16(sA + off, in ? (const void *)(A + (size_t)gm * lda + k0 + ch * 8) : (const void *)A, in ? 16 : 0);
+    }
+#pragma unroll
+    for (int i = 0; i < BN * 8 / 128; i++) {
+        const int v = t + 128 * i;
+        const int row = v >> 3, ch = v & 7;
+        const int off = ((row >> 3) * 8 + ch) * 128 + (row & 7) * 16;
+        const int gn = n0 + row;
+        const bool in = gn < N;
+        cp_async16(sB + off, in ? (const void *)(B + (size_t)gn * ldb + k0 + ch * 8) : (const void *)B, in ? 16 : 0);
+    }
+}
+
+template <int BN>
 __global__ void __launch_bounds__(128) k_gemm_tc(const bf16 *__restrict__ A, int lda, const bf16 *__restrict__ B,
                                                  int ldb, float *__restrict__ C, int ldc, int M, int N, int K,
                                                  int accumulate, int *err, uint32_t wait_iters)
 {
-    __shared__ __align__(1024) unsigned char sA[GT_M * GT_K * 2];
-    __shared__ __align__(1024) unsigned char sB[GT_N * GT_K * 2];
-    __shared__ __align__(8) uint64_t bar;
+    using G = GemmShape<BN>;
+    constexpr int S = GT_STAGES;
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    __shared__ __align__(8) uint64_t bar[S];
     __shared__ uint32_t tmem_base;
-    __shared__ int failed;
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-    const int m0 = blockIdx.x * GT_M, n0 = blockIdx.y * GT_N;
+    const int m0 = blockIdx.x * GT_M, n0 = blockIdx.y * BN;
+    const int nk = K / GT_K;
     if (w == 0) {
-        tc::tmem_alloc(&tmem_base, 128);
+        tc::tmem_alloc(&tmem_base, BN);
         tc::tmem_relinquish();
     }
     if (t == 0) {
-        tc::mbar_init(&bar, 1);
-        failed = 0;
+        for (int i = 0; i < S; i++) tc::mbar_init(&bar[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // prologue: slices 0 .. S-2 in flight (one commit group per slice; empty groups past the end)
+#pragma unroll
+    for (int st = 0; st < S - 1; st++) {
+        if (st < nk)
+            gemm_load_slice<BN>(gsm + st * G::STAGE, gsm + st * G::STAGE + G::A_BYTES, A, lda, B, ldb, M, N, m0, n0,
+                                st, t);
+        cp_async_commit();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = tmem_base;
-    const uint32_t idesc = tc::idesc_bf16_f32(GT_M, GT_N);
-    uint32_t phase = 0;
-    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
-    for (int k0 = 0; k0 < K; k0 += GT_K) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int v = t + 128 * i;
-            const int row = v >> 3, ch = v & 7;
-            const int off = ((row >> 3) * 8 + ch) * 128 + (row & 7) * 16;
-            const int gm = m0 + row, gn = n0 + row;
-            uint4 a = zero, b = zero;
-            if (gm < M) a = *reinterpret_cast<const uint4 *>(A + (size_t)gm * lda + k0 + ch * 8);
-            if (gn < N) b = *reinterpret_cast<const uint4 *>(B + (size_t)gn * ldb + k0 + ch * 8);
-            *reinterpret_cast<uint4 *>(sA + off) = a;
-            *reinterpret_cast<uint4 *>(sB + off) = b;
-        }
-        tc::fence_proxy_async_smem();
-        __syncthreads();
+    const uint32_t idesc = tc::idesc_bf16_f32(GT_M, BN);
+    bool ok = true;
+    int issued = -1; // last slice whose MMAs were committed
+    for (int i = 0; i < nk; i++) {
+        cp_async_wait<S - 2>();            // this thread's copies of slice i have landed
+        tc::fence_proxy_async_smem();      // ... and are visible to the tensor core
+        if (__syncthreads_or(!ok)) break;  // every thread's copies of slice i, unless a wait gave up
+        const int st = i % S;
         if (t == 0) {
             tc::fence_after_sync();
-            const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+            const uint32_t a0 = tc::smem_u32(gsm + st * G::STAGE), b0 = a0 + G::A_BYTES;
 #pragma unroll
             for (int s = 0; s < GT_K / 16; s++) {
                 const uint64_t ad = tc::smem_desc_kmajor(a0 + 256u * s, 128u, 1024u);
                 const uint64_t bd = tc::smem_desc_kmajor(b0 + 256u * s, 128u, 1024u);
-                tc::mma_bf16(tbase, ad, bd, idesc, (k0 > 0 || s > 0) ? 1u : 0u);
+                tc::mma_bf16(tbase, ad, bd, idesc, (i > 0 || s > 0) ? 1u : 0u);
             }
-            tc::mma_commit(&bar);
+            tc::mma_commit(&bar[st]);
         }
-        if (!tc::mbar_wait_bounded(&bar, phase, wait_iters)) failed = 1;
-        phase ^= 1u;
-        __syncthreads();
-        if (failed) break;
+        issued = i;
+        // slice i + S - 1 goes into the stage that slice i - 1 used: wait for those MMAs first
+        const int nxt = i + S - 1;
+        if (nxt < nk) {
+            if (i >= 1 && !tc::mbar_wait_bounded(&bar[(i - 1) % S], (uint32_t)((i - 1) / S) & 1u, wait_iters))
+                ok = false;
+            if (ok)
+                gemm_load_slice<BN>(gsm + (nxt % S) * G::STAGE, gsm + (nxt % S) * G::STAGE + G::A_BYTES, A, lda, B,
+                                    ldb, M, N, m0, n0, nxt, t);
+        }
+        cp_async_commit();
     }
+    // the last commit covers every MMA issued before it
+    if (ok && issued == nk - 1 && nk > 0 &&
+        !tc::mbar_wait_bounded(&bar[issued % S], (uint32_t)(issued / S) & 1u, wait_iters))
+        ok = false;
+    const bool failed = __syncthreads_or(!ok) != 0;
+    cp_async_wait_all();
     tc::fence_after_sync();
     if (!failed) {
         const int row = m0 + 32 * w + lane;
 #pragma unroll 1
-        for (int c0 = 0; c0 < GT_N; c0 += 16) {
+        for (int c0 = 0; c0 < BN; c0 += 16) {
             float v[16];
             tc::tmem_ld16(tbase + ((uint32_t)(32 * w) << 16) + (uint32_t)c0, v);
             if (row < M) {
@@ -116,20 +178,35 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16 *__restrict__ A, int
         }
     } else {
         if (t == 0) atomicOr(err, 1);
-        // the commit in flight (always the full bound, so the MMAs are done
-        // before their TMEM is freed)
-        tc::mbar_wait_bounded(&bar, phase ^ 1u, kWaitIters);
+        // the MMAs in flight finish before their TMEM is freed (full bound)
+        if (issued >= 0) tc::mbar_wait_bounded(&bar[issued % S], (uint32_t)(issued / S) & 1u, kWaitIters);
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (w == 0) tc::tmem_dealloc(tbase, 128);
+    if (w == 0) tc::tmem_dealloc(tbase, BN);
 }
+
+static bool g_gemm_attr = false;
 
 void gemm_tc(const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, int M, int N, int K, int accumulate,
              int *err, cudaStream_t s)
 {
-    dim3 g((M + GT_M - 1) / GT_M, (N + GT_N - 1) / GT_N);
-    k_gemm_tc<<<g, 128, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate, err, g_wait_iters);
+    if (!g_gemm_attr) {
+        cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmShape<128>::SMEM);
+        cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmShape<64>::SMEM);
+        g_gemm_attr = true;
+    }
+    const int mt = (M + GT_M - 1) / GT_M;
+    // 128-wide tiles when they give at least two tiles per SM, else 64-wide (twice the CTAs)
+    if ((long long)mt * ((N + 127) / 128) >= 2 * 148) {
+        dim3 g(mt, (N + 127) / 128);
+        k_gemm_tc<128><<<g, 128, GemmShape<128>::SMEM, s>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate, err,
+                                                            g_wait_iters);
+    } else {
+        dim3 g(mt, (N + 63) / 64);
+        k_gemm_tc<64><<<g, 128, GemmShape<64>::SMEM, s>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate, err,
+                                                          g_wait_iters);
+    }
 }
 
 } // namespace lcmc

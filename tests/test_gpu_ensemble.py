@@ -9,7 +9,10 @@ the same Boltzmann distribution with a different move schedule; 16 replicas
 from the same lattice start, each with its own seed, give means whose
 standard error comes from the spread of the replica means.  Both must agree
 within 3 combined standard errors, for the FP32 kernel (the production path)
-and the FP64 kernel.
+and the FP64 kernel.  The lattice start relaxes slowly: means over blocks of
+1000 sweeps from sweep 200 on (16 replicas, both kernels) run -0.777, -0.750,
+-0.746 and then stay within 0.001 of -0.7452, so the production sweeps start
+after a burn-in of 5000.
 """
 import numpy as np
 import pytest
@@ -19,7 +22,7 @@ from parellel_mc_mpi_for_liquidcrystalsystems_b200 import da
 
 pytestmark = pytest.mark.gpu
 
-REPLICAS, BURN, SWEEPS = 16, 1000, 3000
+REPLICAS, BURN, SWEEPS = 16, 5000, 4000
 
 
 @pytest.mark.parametrize("precision", [1, 0])

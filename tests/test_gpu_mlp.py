@@ -35,7 +35,9 @@ def fp(a):
     return a.ctypes.data_as(FP)
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 128, 256), (300, 200, 4224), (128, 4224, 512)])
+# the last shape is the surrogate's first layer on a training batch of 8192 samples
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 128, 256), (300, 200, 4224), (128, 4224, 512),
+                                   (8192, 128, 4224)])
 def test_gemm_tensor_cores(M, N, K):
     rng = np.random.default_rng(M + N + K)
     A = rng.normal(size=(M, K)).astype(np.float32)

@@ -4,8 +4,9 @@ For callers that cannot let this library allocate device memory (their own
 pool owns the GPU, or their time step cannot take the device-wide
 synchronisation of cudaMalloc/cudaFree): the energy of a configuration the
 caller holds in device memory, computed with a fixed scratch area inside
-liblcmc.so.  Checked here through the C ABI against the allocating entry point
-(lcmc_total_energy) within the 1e-12 relative tolerance of the other energy
+liblcmc.so.  Checked here through the C ABI against the CPU oracle's FP64
+total energy (canonical arithmetic) and against the allocating entry point
+(lcmc_total_energy), within the 1e-12 relative tolerance of the other energy
 tests, on two calls in a row, plus the size limit.
 
 This file is collected last on purpose, so that a run stopping at the first
@@ -14,6 +15,7 @@ failure has already run every other test.
 import ctypes as C
 
 import numpy as np
+import oracle_ctypes as oc
 import pytest
 
 import parellel_mc_mpi_for_liquidcrystalsystems_b200 as lcmc
@@ -68,6 +70,24 @@ def test_noalloc_total_energy_matches_allocating_entry_point():
     rc, _ = _noalloc(torch, p, state, box, out, stream)
     torch.cuda.synchronize()
     assert float(out.item()) == first
+
+
+@pytest.mark.parametrize("n,R", [(1000, 0.0), (6000, 3.0)])
+def test_noalloc_total_energy_matches_oracle(n, R):
+    """The allocation-free energy against the oracle's FP64 cell-list total of
+    the same state (tot_ene, MCnptColloid.c:1598-1622, canonical arithmetic)."""
+    torch = pytest.importorskip("torch")
+    kw = dict(colloid_radius=R, colloid_wall_option=1) if R > 0 else {}
+    p, state, box, _ = _config(n, 0.30, 9, 2, **kw)
+    op = oc.params(num_particles=n, system_density=0.30, rng_seed=9, **COMMON, **kw)
+    want = oc.total_energy(oc.consts(op, oc.ARITH_CANONICAL), [np.ascontiguousarray(a) for a in state],
+                           np.ascontiguousarray(box, dtype=np.float64))
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    rc, _ = _noalloc(torch, p, state, box, out, torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    got = float(out.item())
+    assert abs(got - want) <= 1e-12 * abs(want), (got, want)
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit():
