@@ -48,7 +48,8 @@ WORKLOAD = {
                 "lattice start (body-centred tetragonal, layers 1.05 sigma_ee apart along z) with orientations "
                 "within 20 deg of z",
     "n_particles": N_PART,
-    "precision": "fp32 pair terms, fp64 state and sums",
+    # timing hygiene of the GPU arm (both arms print this same config)
+    "l2": "GPU arm: L2 flushed between timed sweeps (256 MiB memset)",
 }
 
 
@@ -271,9 +272,10 @@ def kernel_traffic():
     k_phase_fast launch on this workload and where the figure comes from: a
     fixed ncu capture (ncu cannot run inside the timed process), so it is
     the same in every run and is refreshed when the kernel changes."""
-    return 44.0064e6 + 0.949504e6, ("fixed, from one ncu --set full capture of k_phase_fast launches 17-18 of "
-                                    "`bench.py --steps 3 --warmup 3 --e2e-steps 1 --cpu-seconds 2 --da-sweeps 0` "
-                                    "(44.0 MB read + 0.95 MB written per launch); not measured in this run")
+    return 45.368576e6 + 1.271808e6, ("fixed, from one ncu --set full capture of k_phase_fast launches 265-266 "
+                                      "of `bench.py --steps 3 --warmup 3 --e2e-steps 1 --cpu-seconds 2 "
+                                      "--port-seconds 0 --da-sweeps 0 --jammed-steps 0 --batch-steps 0` (45.4 MB "
+                                      "read + 1.3 MB written per launch); not measured in this run")
 
 
 # ---------------------------------------------------------------------------
@@ -363,18 +365,18 @@ def npt_da(lcmc, torch, sweeps, train_sweeps):
     # the N = 262,144 system: compress from a dilute start, settle at dlnV_max
     # 0.01, then every arm from that one state with one seed
     n = 262144
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05, 56)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 11, 0.05, 48)) as s:
         st, box = dilute_start(n, 0.06, 8.0, 12)
         s.upload(*st, box)
         s.sweep(1000)
         st4, box4 = s.download()
-    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 13, 0.01, 56)) as s:
+    with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 13, 0.01, 48)) as s:
         s.upload(*st4, box4)
         s.sweep(1000)
         st4, box4 = s.download()
     arms = {}
     for name in ("plain", "learned", "fp32_screen"):
-        with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01, 56)) as s:
+        with lcmc.GBSystem(npt_params(lcmc, n, 0.85, 2.0, 8.0, 21, 0.01, 48)) as s:
             s.upload(*st4, box4)
             if name == "learned":
                 s.set_surrogate(sur)
@@ -739,9 +741,10 @@ def main():
                 "steps": steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded body-centred lattice, the GPU arm's start)",
-                "config": dict(WORKLOAD, parallelism="cpu openmp", precision="fp64 (the reference's own code)",
-                               step=f"a bounded sample of {res['attempts_per_step']} consecutive attempts of the "
-                                    f"N={N_PART} system (a sweep is {N_PART} attempts)"),
+                "config": dict(WORKLOAD),
+                "arm": {"parallelism": "cpu openmp", "precision": "fp64 (the reference's own code)",
+                        "step": f"a bounded sample of {res['attempts_per_step']} consecutive attempts of the "
+                                f"N={N_PART} system (a sweep is {N_PART} attempts)"},
                 "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -862,11 +865,12 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded lattice, relaxing from the lattice start)",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single system",
-                       l2="flushed between sweeps (256 MiB memset)",
-                       timed_window=f"sweeps {args.relax_sweeps + max(3, args.warmup) + 1}-"
-                                    f"{args.relax_sweeps + max(3, args.warmup) + args.steps} of the run from the "
-                                    "lattice start"),
+        "config": dict(WORKLOAD),
+        "arm": {"parallelism": f"replicas x{world}" if world > 1 else "single system",
+                "precision": "fp32 pair terms, fp64 state and sums",
+                "timed_window": f"sweeps {args.relax_sweeps + max(3, args.warmup) + 1}-"
+                                f"{args.relax_sweeps + max(3, args.warmup) + args.steps} of the run from the "
+                                "lattice start"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * N_PART + 24 + 8,
                 "d2h_bytes_per_step": 6 * 8 * N_PART + 24 + 8,
                 "step": "lcmc_upload_with_energy (pinned host SoA, caller-carried energy) + lcmc_sweep + "

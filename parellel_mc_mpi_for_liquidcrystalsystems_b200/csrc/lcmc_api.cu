@@ -605,10 +605,13 @@ static int capacity_rule(const lcmc_params &p, double L, double wmin, bool npt)
     cell_count_stats(p, L, wmin, &mean, &sd);
     // a cell above the capacity is attempted in FP64 (correct, only slower),
     // so the rule sizes for the liquid, not for the lattice start's fullest
-    // cells or rare fluctuations: 4 standard deviations, + 4
-    int want = (int)std::ceil(mean + 4.0 * sd + 4.0);
-    if (npt) want = std::max(want, fast_variant(1).amax);
-    return want;
+    // cells or rare fluctuations: 4 standard deviations, + 4.  NPT systems
+    // get no larger class by default (the classes with more CTAs per SM are
+    // the faster ones): a box that compresses far below its creation volume
+    // fills its cells beyond the rule, and its over-full cells are attempted
+    // in FP64; cell_capacity or lcmc_autotune chooses a larger class
+    (void)npt;
+    return (int)std::ceil(mean + 4.0 * sd + 4.0);
 }
 
 // the smallest capacity class that holds `want` (else the largest)

@@ -215,8 +215,13 @@ __device__ __noinline__ void fixup_big(const DevView *__restrict__ vp, int r, in
         const double op[3] = {v.px[gp], v.py[gp], v.pz[gp]}, up[3] = {v.ox[gp], v.oy[gp], v.oz[gp]};
         const double np_[3] = {v.tnx[gp], v.tny[gp], v.tnz[gp]}, wp[3] = {v.tux[gp], v.tuy[gp], v.tuz[gp]};
         // A = (o_q, o_p), B = (n_q, o_p), C = (o_q, n_p), D = (n_q, n_p)
-        const double term[4] = {term64<SPEC21>(p, op, up, oq, uq), term64<SPEC21>(p, op, up, nq, wq),
-                                term64<SPEC21>(p, np_, wp, oq, uq), term64<SPEC21>(p, np_, wp, nq, wq)};
+        double term[4] = {term64<SPEC21>(p, op, up, oq, uq), term64<SPEC21>(p, op, up, nq, wq),
+                          term64<SPEC21>(p, np_, wp, oq, uq), term64<SPEC21>(p, np_, wp, nq, wq)};
+        // terms with the trial state of a particle that cannot move are never used
+        const bool hp = sm.hard[pp] != 0, hq = sm.hard[q] != 0;
+        if (hq) term[1] = term[3] = 0.0;
+        if (hp) term[2] = term[3] = 0.0;
+        if (hp && hq) term[0] = 0.0;
         if (!(fabs(term[0]) <= 1e5 && fabs(term[1]) <= 1e5 && fabs(term[2]) <= 1e5 && fabs(term[3]) <= 1e5)) {
             sm.big = 1;
         } else {
@@ -585,6 +590,13 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(c
                         D = pair_fast_t<SPEC21>(K, dx, dy, dz, r2, R2.y, R2.z, R2.w, Q2.y, Q2.z, Q2.w);
                         D = r2 < K.rc2 ? D : 0.0f;
                     }
+                    // a particle that cannot move (colloid hard core, or a trial out of the cell) keeps
+                    // its old state: terms with its trial state are never used, so they are dropped
+                    // before the size test (p hard: C and D unused; q hard: B and D unused)
+                    const bool hp = sm.hard[pp] != 0, hq = sm.hard[q] != 0;
+                    if (hq) B = D = 0.0f;
+                    if (hp) Cc = D = 0.0f;
+                    if (hp && hq) A = 0.0f;
                     if (!(fabsf(A) <= K.big && fabsf(B) <= K.big && fabsf(Cc) <= K.big && fabsf(D) <= K.big)) {
                         const int slot = atomicAdd(&sm.nbigp, 1); // the fix-up pass rewrites this pair
                         if (slot < SM::BIGCAP) sm.bigp[slot] = (unsigned short)idx;
