@@ -4,6 +4,8 @@
 // tensor cores (tcgen05.mma, accumulators in TMEM); bias, activation, loss and
 // Adam are small FP32 CUDA-core kernels.  (No reference counterpart: the
 // reference has no NPT move at all, MCnptColloid.c:3978.)
+#include <cuda.h> // CUtensorMap and its enums (the encoder is taken from the driver at run time)
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -186,6 +188,179 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const bf16 *__restrict__ A, int
     if (w == 0) tc::tmem_dealloc(tbase, BN);
 }
 
+// ---------------------------------------------------------------------------
+// The same product with TMA tile loads (used when A and B are 16-byte aligned
+// with 16-byte row strides): one thread streams 64-wide K slices of A
+// (128 rows) and B (BN rows) through GT_TMA_STAGES shared-memory stages with
+// cp.async.bulk.tensor (128-byte swizzle, rows beyond M or N filled with
+// zeros), each stage's loads completing on its "full" mbarrier; the same
+// thread issues the slice's four MMAs once the stage is full and commits them
+// to the stage's "empty" mbarrier, and refills the stage the previous slice
+// used as soon as that slice's MMAs have completed, so the loads of the next
+// GT_TMA_STAGES - 1 slices are in flight while the tensor core works.  The
+// other threads wait at a block barrier for the epilogue.  Every wait is
+// bounded; on a timeout the tile sets *err, waits (with the full bound) for its
+// loads and MMAs in flight and frees its TMEM.
+// ---------------------------------------------------------------------------
+constexpr int GT_TMA_STAGES = 4;
+template <int BN> struct TmaShape {
+    static constexpr int A_BYTES = GT_M * GT_K * 2, B_BYTES = BN * GT_K * 2, STAGE = A_BYTES + B_BYTES;
+    static constexpr int SMEM = GT_TMA_STAGES * STAGE + 1024; // + slack to align the stages to 1024 bytes
+};
+
+// K slice j of A (128 rows from m0) and B (rows from n0) into one stage, on its full barrier.
+__device__ __forceinline__ void tma_stage_load(unsigned char *dst, int a_bytes, uint32_t stage_bytes,
+                                               const CUtensorMap *ta, const CUtensorMap *tb, int j, int m0, int n0,
+                                               uint64_t *full)
+{
+    tc::mbar_arrive_expect_tx(full, stage_bytes);
+    tc::tma_load_2d(dst, ta, j * GT_K, m0, full);
+    tc::tma_load_2d(dst + a_bytes, tb, j * GT_K, n0, full);
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_gemm_tma(const __grid_constant__ CUtensorMap ta,
+                                                  const __grid_constant__ CUtensorMap tb, float *__restrict__ C,
+                                                  int ldc, int M, int N, int K, int accumulate, int *err,
+                                                  uint32_t wait_iters)
+{
+    using G = TmaShape<BN>;
+    constexpr int S = GT_TMA_STAGES;
+    extern __shared__ unsigned char gsm_raw[];
+    __shared__ __align__(8) uint64_t full[S], empty[S];
+    __shared__ uint32_t tmem_base;
+    __shared__ int bad;
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+    const int m0 = blockIdx.x * GT_M, n0 = blockIdx.y * BN;
+    const int nk = K / GT_K;
+    const uint32_t raw = tc::smem_u32(gsm_raw);
+    unsigned char *gsm = gsm_raw + (((raw + 1023u) & ~1023u) - raw);
+    if (w == 0) {
+        tc::tmem_alloc(&tmem_base, BN);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        for (int i = 0; i < S; i++) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+    if (t == 0) {
+        const uint32_t idesc = tc::idesc_bf16_f32(GT_M, BN);
+        int last_load[S]; // last slice loaded into each stage (-1: none)
+#pragma unroll
+        for (int i = 0; i < S; i++) last_load[i] = -1;
+        for (int j = 0; j < S && j < nk; j++) {
+            tma_stage_load(gsm + j * G::STAGE, G::A_BYTES, (uint32_t)G::STAGE, &ta, &tb, j, m0, n0, &full[j]);
+            last_load[j] = j;
+        }
+        bool ok = true;
+        int issued = -1; // last slice whose MMAs were committed
+        for (int i = 0; i < nk; i++) {
+            const int st = i % S;
+            if (!tc::mbar_wait_bounded(&full[st], (uint32_t)(i / S) & 1u, wait_iters)) {
+                ok = false;
+                break;
+            }
+            tc::fence_after_sync();
+            const uint32_t a0 = tc::smem_u32(gsm + st * G::STAGE), b0 = a0 + G::A_BYTES;
+#pragma unroll
+            for (int s = 0; s < GT_K / 16; s++)
+                tc::mma_bf16(tbase, tc::smem_desc_sw128(a0 + 32u * s), tc::smem_desc_sw128(b0 + 32u * s), idesc,
+                             (i > 0 || s > 0) ? 1u : 0u);
+            tc::mma_commit(&empty[st]);
+            issued = i;
+            // refill the stage that slice i - 1 used once its MMAs have completed
+            const int j = i - 1 + S;
+            if (i >= 1 && j < nk) {
+                const int ps = (i - 1) % S;
+                if (!tc::mbar_wait_bounded(&empty[ps], (uint32_t)((i - 1) / S) & 1u, wait_iters)) {
+                    ok = false;
+                    break;
+                }
+                tma_stage_load(gsm + ps * G::STAGE, G::A_BYTES, (uint32_t)G::STAGE, &ta, &tb, j, m0, n0,
+                               &full[ps]);
+                last_load[ps] = j;
+            }
+        }
+        // the last commit covers every MMA issued before it
+        if (ok && issued >= 0 &&
+            !tc::mbar_wait_bounded(&empty[issued % S], (uint32_t)(issued / S) & 1u, wait_iters))
+            ok = false;
+        if (!ok || issued != nk - 1) {
+            bad = 1;
+            atomicOr(err, 1);
+            // loads and MMAs in flight finish before the block leaves (full bound)
+            for (int st = 0; st < S; st++)
+                if (last_load[st] >= 0)
+                    tc::mbar_wait_bounded(&full[st], (uint32_t)(last_load[st] / S) & 1u, kWaitIters);
+            if (issued >= 0) tc::mbar_wait_bounded(&empty[issued % S], (uint32_t)(issued / S) & 1u, kWaitIters);
+        }
+    }
+    __syncthreads();
+    tc::fence_after_sync();
+    if (!bad) {
+        const int row = m0 + 32 * w + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tbase + ((uint32_t)(32 * w) << 16) + (uint32_t)c0, v);
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int col = n0 + c0 + j;
+                    if (col < N) {
+                        float *p = C + (size_t)row * ldc + col;
+                        *p = accumulate ? *p + v[j] : v[j];
+                    }
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (w == 0) tc::tmem_dealloc(tbase, BN);
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static int g_encode_state = 0; // 0 unknown, 1 available, -1 not available
+
+static bool tma_available()
+{
+    if (g_encode_state == 0) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && fn) {
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+            g_encode_state = 1;
+        } else {
+            cudaGetLastError();
+            g_encode_state = -1;
+        }
+    }
+    return g_encode_state == 1;
+}
+
+// rows x K BF16 matrix with row stride ld elements, tiles of box_rows x 64
+static bool make_tile_map(CUtensorMap *m, const bf16 *p, int rows, int K, int ld, int box_rows)
+{
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2u};
+    const cuuint32_t box[2] = {(cuuint32_t)GT_K, (cuuint32_t)box_rows};
+    const cuuint32_t es[2] = {1u, 1u};
+    return g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(p), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 static bool g_gemm_attr = false;
 
 void gemm_tc(const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, int M, int N, int K, int accumulate,
@@ -194,11 +369,30 @@ void gemm_tc(const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, 
     if (!g_gemm_attr) {
         cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmShape<128>::SMEM);
         cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmShape<64>::SMEM);
+        cudaFuncSetAttribute(k_gemm_tma<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TmaShape<128>::SMEM);
+        cudaFuncSetAttribute(k_gemm_tma<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TmaShape<64>::SMEM);
         g_gemm_attr = true;
     }
     const int mt = (M + GT_M - 1) / GT_M;
     // 128-wide tiles when they give at least two tiles per SM, else 64-wide (twice the CTAs)
-    if ((long long)mt * ((N + 127) / 128) >= 2 * 148) {
+    const bool wide = (long long)mt * ((N + 127) / 128) >= 2 * 148;
+    if (K >= GT_K && tma_available() && ((uintptr_t)A & 15u) == 0 && ((uintptr_t)B & 15u) == 0 && lda % 8 == 0 &&
+        ldb % 8 == 0) {
+        CUtensorMap ta, tb;
+        if (make_tile_map(&ta, A, M, K, lda, GT_M) && make_tile_map(&tb, B, N, K, ldb, wide ? 128 : 64)) {
+            if (wide) {
+                dim3 g(mt, (N + 127) / 128);
+                k_gemm_tma<128><<<g, 128, TmaShape<128>::SMEM, s>>>(ta, tb, C, ldc, M, N, K, accumulate, err,
+                                                                    g_wait_iters);
+            } else {
+                dim3 g(mt, (N + 63) / 64);
+                k_gemm_tma<64><<<g, 128, TmaShape<64>::SMEM, s>>>(ta, tb, C, ldc, M, N, K, accumulate, err,
+                                                                  g_wait_iters);
+            }
+            return;
+        }
+    }
+    if (wide) {
         dim3 g(mt, (N + 127) / 128);
         k_gemm_tc<128><<<g, 128, GemmShape<128>::SMEM, s>>>(A, lda, B, ldb, C, ldc, M, N, K, accumulate, err,
                                                             g_wait_iters);

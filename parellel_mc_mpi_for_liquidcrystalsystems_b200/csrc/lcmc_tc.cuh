@@ -80,6 +80,38 @@ __device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t saddr, uint32_t lb
     return d;
 }
 
+// K-major operand in the 128-byte swizzled layout that a TMA tile load with
+// CU_TENSOR_MAP_SWIZZLE_128B writes: rows of 128 bytes (64 BF16 of K), 16-byte
+// chunks XOR-permuted by the row index mod 8, 8-row groups 1024 bytes apart
+// (SBO); LBO is unused by this layout (1).  The tile must start on a 1024-byte
+// boundary; the k-th 16-wide K step of an MMA starts 32 k bytes further.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;             // LBO (unused)
+    d |= (uint64_t)(1024u >> 4) << 32;  // SBO: 8-row groups
+    d |= (uint64_t)1 << 46;             // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;             // layout type: 128-byte swizzle
+    return d;
+}
+
+// ---- TMA (no multicast) ----
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// 2-D tile of the tensor map at (x = innermost element index, y = row) into
+// shared memory; its bytes complete on the mbarrier's transaction count.
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *tmap, int x, int y, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 // Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major, dense.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N)
 {
