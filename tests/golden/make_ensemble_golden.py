@@ -22,8 +22,9 @@ production run as a stationarity check.
 `make_ensemble_golden.py part K` runs the gas chain with seed SEED + K into
 ensemble_part_K.npz (independent chains can run on separate cores), and
 `make_ensemble_golden.py combine K1 K2 ...` merges those parts with the main
-chain into ensemble_golden.npz: the mean over every chain's blocks, with the
-standard error of all blocks taken together.
+chain into ensemble_golden.npz: the mean of the chain means, with the
+standard error from their spread (ensemble_golden.npz holds 12 chains:
+combine 1 2 ... 11).
 
 `make_ensemble_golden.py dense` writes ensemble_dense_golden.npz instead: the
 dense liquid of the CPU-runnable configuration (N = 1000, rho* = 0.30,
@@ -127,23 +128,26 @@ def compressed_start(oc, n, rho, T, R, seed):
 
 
 def combine(parts):
-    """The main chain (ensemble_golden.npz, its u/p2 series every 10 sweeps
-    and its block means) plus independent chains ensemble_part_K.npz: every
-    chain cut into BLOCKS blocks; the golden mean is the mean of all blocks and
-    its standard error the blocks' spread over the square root of their count."""
+    """The main chain (ensemble_golden.npz, its u/p2 series every 10 sweeps)
+    plus independent chains ensemble_part_K.npz: the golden mean is the mean
+    of the chain means and its standard error their spread over the square
+    root of the number of chains (P2 in particular drifts slowly, so blocks
+    inside one chain are not independent enough to give the error)."""
     main_f = os.path.join(HERE, "ensemble_golden.npz")
     files = [main_f] + [os.path.join(HERE, f"ensemble_part_{k}.npz") for k in parts]
-    bu, bp = [], []
+    cu, cp = [], []
     for f in files:
         g = np.load(f)
-        for v, dst in ((g["u_series"], bu), (g["p2_series"], bp)):
-            dst.extend(x.mean() for x in np.array_split(np.asarray(v), int(g["blocks"])))
+        cu.append(float(np.mean(g["u_series"])))
+        cp.append(float(np.mean(g["p2_series"])))
     g = dict(np.load(main_f))
-    g["u_mean"], g["u_se"] = float(np.mean(bu)), float(np.std(bu, ddof=1) / np.sqrt(len(bu)))
-    g["p2_mean"], g["p2_se"] = float(np.mean(bp)), float(np.std(bp, ddof=1) / np.sqrt(len(bp)))
-    g["chains"] = len(files)
+    n = len(files)
+    g["u_mean"], g["u_se"] = float(np.mean(cu)), float(np.std(cu, ddof=1) / np.sqrt(n))
+    g["p2_mean"], g["p2_se"] = float(np.mean(cp)), float(np.std(cp, ddof=1) / np.sqrt(n))
+    g["chains"] = n
+    g["chain_u"], g["chain_p2"] = np.array(cu), np.array(cp)
     np.savez(main_f, **g)
-    print(f"{len(files)} chains: U/N = {g['u_mean']:.6f} +- {g['u_se']:.6f}  P2 = {g['p2_mean']:.6f} +- "
+    print(f"{n} chains: U/N = {g['u_mean']:.6f} +- {g['u_se']:.6f}  P2 = {g['p2_mean']:.6f} +- "
           f"{g['p2_se']:.6f} -> {main_f}")
 
 

@@ -1,7 +1,7 @@
 """Ensemble averages against the reference's own Monte Carlo chain.
 
 tests/golden/ensemble_golden.npz holds <U/N> and <P2> (block-averaged, with
-standard errors; five independent chains) of runs of the reference's attempt_monte_carlo_move
+standard errors from the spread of twelve independent chains) of runs of the reference's attempt_monte_carlo_move
 (MCnptColloid.c:2445-2604, random particle per attempt) on N = 1728 rods at
 rho* = 0.10, T* = 2.0, step 0.5 and rotation 0.3, with a colloid of radius 2
 (made by tests/golden/make_ensemble_golden.py).  The checkerboard sweeps here sample
