@@ -178,12 +178,12 @@ def test_npt_running_energy_tracks_the_recompute():
         assert abs(st["energy"] - e) <= 1e-6 * (abs(e) + n)
 
 
-def _batch_params():
+def _batch_params(precision=1):
     """Small boxes on the fine cell grid (odd counts allowed): 5, 6 and 7 cells
     of about 4.7 per axis instead of 4, 6 and 6 cells up to 5.9 wide, so each
     replica keeps the FP32 kernel; NVT, NPT and a colloid replica."""
     common = dict(gb_kappa=3.0, gb_kappa_prime=5.0, gb_mu_exponent=2.0, gb_nu_exponent=1.0, cutoff_radius=4.0,
-                  max_displacement=0.1, max_rotation=0.1, precision_mode=1, cell_grid=1,
+                  max_displacement=0.1, max_rotation=0.1, precision_mode=precision, cell_grid=1,
                   init_orientation_cone_deg=20.0, init_lattice=1)
     return [
         lcmc.default_params(num_particles=4096, system_density=0.32, system_temperature=0.8, rng_seed=201, **common),
@@ -194,17 +194,19 @@ def _batch_params():
     ]
 
 
-def test_fine_grid_batch_matches_single_runs_fp32():
-    """Replicas of a batch on the FP32 kernel (fine grid: up to 27 colour
-    phases) reproduce their single runs bit for bit."""
-    ps = _batch_params()
+@pytest.mark.parametrize("precision", [1, 0])
+def test_fine_grid_batch_matches_single_runs(precision):
+    """Replicas of a batch on the fine grid (27 colour phases, of which the
+    6-cell replica uses 8) reproduce their single runs bit for bit, on the FP32
+    and on the FP64 kernel."""
+    ps = _batch_params(precision)
     singles = []
     for p in ps:
         with lcmc.GBSystem(p) as s:
             s.get_initial_config()
             s.sweep(4)
             st = s.stats()
-            assert st["kernel"] == 1, st
+            assert st["kernel"] == precision, st
             singles.append((s.download(), st))
     with lcmc.GBSystem(ps) as b:
         for r in range(len(ps)):
@@ -216,7 +218,7 @@ def test_fine_grid_batch_matches_single_runs_fp32():
                 assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
             assert np.array_equal(got[1].view(np.uint64), want[1].view(np.uint64))
             st = b.stats(r)
-            assert st["accepted"] == wst["accepted"] and st["energy"] == wst["energy"] and st["kernel"] == 1
+            assert st["accepted"] == wst["accepted"] and st["energy"] == wst["energy"] and st["kernel"] == precision
 
 
 def test_fine_grid_fp32_decisions_match_fp64():
@@ -244,3 +246,33 @@ def test_fine_grid_fp32_decisions_match_fp64():
             if np.array_equal(oa, ob):
                 assert np.all(np.abs(ea - eb)[soft] <= 0.02 + 1e-5 * np.abs(eb[soft]))
         assert a.stats()["kernel"] == 1 and b.stats()["kernel"] == 0
+
+
+def test_fp32_npt_ensemble_matches_fp64():
+    """The reference never moves the volume, so the FP32 kernel's NPT ensemble
+    is checked against the FP64 kernel's: 12 independent chains each (N = 6000,
+    P* = 1, T* = 1.2, colloid R = 3, one compressed start), mean volume and
+    energy per particle within 4.5 standard errors of the spread of the chain
+    means."""
+    from parellel_mc_mpi_for_liquidcrystalsystems_b200 import da
+    from test_gpu_screen import NPT, compressed
+    state, box = compressed()
+    res = {}
+    for prec in (0, 1):
+        ps = [lcmc.default_params(num_particles=6000, system_density=0.10, rng_seed=700 + r + 50 * prec,
+                                  npt_max_dlnV=0.01, cell_capacity=64, **dict(NPT, precision_mode=prec))
+              for r in range(12)]
+        with lcmc.GBSystem(ps) as s:
+            for r in range(12):
+                s.upload(*state, box, replica=r)
+            s.sweep(300)
+            s.record_history(2000)
+            s.sweep(2000)
+            vol = np.array([da.p2_series(s, r)[3].mean() for r in range(12)])
+            u = np.array([da.p2_series(s, r)[2].mean() / 6000 for r in range(12)])
+            assert all(s.stats(r)["kernel"] == prec for r in range(12))
+        res[prec] = (vol, u)
+    for i, name in enumerate(("volume", "U/N")):
+        a, b = res[0][i], res[1][i]
+        se = np.hypot(a.std(ddof=1), b.std(ddof=1)) / np.sqrt(len(a))
+        assert abs(a.mean() - b.mean()) < 4.5 * se, (name, a.mean(), b.mean(), se)
