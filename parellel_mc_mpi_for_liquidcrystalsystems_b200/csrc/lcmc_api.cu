@@ -24,6 +24,9 @@ using namespace lcmc;
 
 static thread_local std::string g_create_error;
 
+constexpr int kMaxGroups = 8;
+constexpr int kGroups = 2; // replica groups of a batch of 8 or more replicas (2, 4 and 8 timed alike)
+
 struct lcmc_ctx {
     int R = 0;
     int ntot = 0, ctot = 0;
@@ -46,6 +49,14 @@ struct lcmc_ctx {
     int *d_cell_fp64 = nullptr;
     int *d_p2c = nullptr, *d_resc_count = nullptr, *d_resc_list = nullptr;
     int nphase = 8; // colour phases per sweep (LCMC_MAX_COLOURS with a fine-grid replica)
+    // Replica groups of a batch: the colour phases of each group run on their
+    // own stream (a branch of the sweep graph between the rebin and the
+    // statistics), so the phases of different groups overlap instead of all
+    // replicas waiting for the slowest cell of every phase.
+    int ngroup = 1;
+    int grp_lo[kMaxGroups] = {}, grp_hi[kMaxGroups] = {};
+    cudaStream_t side[kMaxGroups] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kMaxGroups] = {};
     unsigned char *d_outcome = nullptr;
     double *d_rec_dE = nullptr, *d_rec_lu = nullptr; // move records (lcmc_record_moves)
     std::vector<unsigned long long> sweeps; // host mirror of every replica's sweep counter
@@ -498,6 +509,9 @@ static DevView view(const lcmc_ctx *c, int parity)
     v.p2c = c->d_p2c;
     v.resc_count = c->d_resc_count;
     v.nphase = c->nphase;
+    v.r_lo = 0;
+    v.r_hi = c->R;
+    v.ngroup = c->ngroup;
     v.resc_list = c->d_resc_list;
     v.rec_dE = c->d_rec_dE;
     v.rec_lu = c->d_rec_lu;
@@ -537,6 +551,11 @@ static void free_ctx(lcmc_ctx *c)
         if (c->graph[i]) cudaGraphExecDestroy(c->graph[i]);
     for (int i = 0; i < 5; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (int g = 0; g < kMaxGroups; g++) {
+        if (c->side[g]) cudaStreamDestroy(c->side[g]);
+        if (c->ev_join[g]) cudaEventDestroy(c->ev_join[g]);
+    }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     void *ptrs[] = {c->d_rep, c->d_stats, c->d_act_off, c->d_p2r, c->d_id[0], c->d_id[1], c->d_cid, c->d_rank,
                     c->d_perm, c->d_scid, c->d_cell_count, c->d_cell_start, c->d_block_sums, c->d_flag, c->d_cell_e0,
                     c->d_cell_e1, c->d_cell_n0, c->d_cell_n1, c->d_cell_pairs, c->d_cell_cands, c->d_outcome,
@@ -781,6 +800,37 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
             free_ctx(c);
             return set_err(nullptr, LCMC_ECUDA, "event creation failed");
         }
+    // replica groups: batches of 8 or more replicas get kGroups contiguous
+    // groups of about equal particle counts (at least two replicas each)
+    c->ngroup = n >= 8 ? std::min(kGroups, n / 2) : 1;
+    {
+        long long total = 0, acc = 0;
+        for (int r = 0; r < n; r++) total += params[r].num_particles;
+        int g = 0;
+        c->grp_lo[0] = 0;
+        for (int r = 0; r < n && g < c->ngroup - 1; r++) {
+            acc += params[r].num_particles;
+            // close group g once it holds its share, leaving a replica for every later group
+            if (acc * c->ngroup >= total * (g + 1) && n - (r + 1) >= c->ngroup - (g + 1)) {
+                c->grp_hi[g] = r + 1;
+                c->grp_lo[++g] = r + 1;
+            }
+        }
+        c->ngroup = g + 1;
+        c->grp_hi[g] = n;
+    }
+    if (c->ngroup > 1) {
+        if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
+            free_ctx(c);
+            return set_err(nullptr, LCMC_ECUDA, "event creation failed");
+        }
+        for (int g = 1; g < c->ngroup; g++)
+            if (cudaStreamCreateWithFlags(&c->side[g], cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->ev_join[g], cudaEventDisableTiming) != cudaSuccess) {
+                free_ctx(c);
+                return set_err(nullptr, LCMC_ECUDA, "stream creation failed");
+            }
+    }
     ALLOC(c->d_rep, n);
     ALLOC(c->d_stats, n);
     ALLOC(c->d_act_off, c->nphase * (n + 1));
@@ -806,8 +856,8 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     ALLOC(c->d_cell_abs, c->ctot);
     ALLOC(c->d_cell_fp64, c->ctot);
     ALLOC(c->d_p2c, c->ctot);
-    ALLOC(c->d_resc_count, c->nphase);
-    ALLOC(c->d_resc_list, (size_t)c->nphase * c->ctot);
+    ALLOC(c->d_resc_count, c->nphase * c->ngroup);
+    ALLOC(c->d_resc_list, (size_t)c->nphase * c->ngroup * c->ctot);
     ALLOC(c->d_outcome, c->ntot);
     ALLOC(c->d_pe0, c->ntot);
     ALLOC(c->d_pe1, c->ntot);
@@ -840,7 +890,7 @@ extern "C" int lcmc_create_batch(const lcmc_params *params, int n, lcmc_ctx **ou
     for (int r = 0; r < n; r++)
         for (int i = 0; i < c->rep[r].nc_max * c->rep[r].nc_max * c->rep[r].nc_max; i++) p2c[c->rep[r].cell_off + i] = r;
     cudaMemcpy(c->d_p2c, p2c.data(), sizeof(int) * c->ctot, cudaMemcpyHostToDevice);
-    cudaMemset(c->d_resc_count, 0, sizeof(int) * c->nphase);
+    cudaMemset(c->d_resc_count, 0, sizeof(int) * c->nphase * c->ngroup);
     cudaMemset(c->d_stats, 0, sizeof(DevStats) * n);
     cudaMemset(c->d_outcome, 0, c->ntot);
     cudaMemset(c->d_cell_e0, 0, sizeof(double) * c->ctot);
@@ -929,13 +979,26 @@ static void enqueue_sweep(lcmc_ctx *c, int parity)
     enqueue_rebin(c, parity);
     cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal);
     DevView v = view(c, parity ^ 1);
-    for (int ci = 0; ci < c->nphase; ci++) {
-        if (c->any_exact) launch_phase_exact(v, c->stream, ci, c->grid_exact);
-        if (c->any_fast) {
-            launch_phase_fast(c->fast_variant, v, c->stream, ci, c->grid_fast);
-            launch_phase_rescue(c->fast_variant & 1, v, c->stream, ci, c->sms);
+    if (c->ngroup > 1) cudaEventRecord(c->ev_fork, c->stream);
+    for (int g = 0; g < c->ngroup; g++) {
+        // group g's phases: its replicas' cells, its own hand-over lists, its own stream
+        DevView vg = v;
+        vg.r_lo = c->grp_lo[g];
+        vg.r_hi = c->grp_hi[g];
+        vg.resc_count = c->d_resc_count + (size_t)g * c->nphase;
+        vg.resc_list = c->d_resc_list + (size_t)g * c->nphase * c->ctot;
+        cudaStream_t sg = g == 0 ? c->stream : c->side[g];
+        if (g > 0) cudaStreamWaitEvent(sg, c->ev_fork, 0);
+        for (int ci = 0; ci < c->nphase; ci++) {
+            if (c->any_exact) launch_phase_exact(vg, sg, ci, c->grid_exact);
+            if (c->any_fast) {
+                launch_phase_fast(c->fast_variant, vg, sg, ci, c->grid_fast);
+                launch_phase_rescue(c->fast_variant & 1, vg, sg, ci, c->sms);
+            }
         }
+        if (g > 0) cudaEventRecord(c->ev_join[g], sg);
     }
+    for (int g = 1; g < c->ngroup; g++) cudaStreamWaitEvent(c->stream, c->ev_join[g], 0);
     cudaEventRecordWithFlags(c->ev[2], c->stream, cudaEventRecordExternal);
     launch_sweep_stats(v, c->stream);
     if (c->any_npt) {
@@ -1141,10 +1204,11 @@ extern "C" int lcmc_get_stream(lcmc_ctx *ctx, void **stream)
 extern "C" int lcmc_kernels_per_sweep(lcmc_ctx *ctx)
 {
     if (!ctx) return LCMC_EINVAL;
-    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases (FP32: with the FP64 hand-over kernel); statistics: chunk sums, sums; volume: propose,
+    // rebin: setup, bin, 3 scan, scatter, sort, gather; phases, per replica group (FP32: with the FP64 hand-over
+    // kernel); statistics: chunk sums, sums; volume: propose,
     // energy, chunk sums, accept, scale; surrogate: 2 feature kernels, 2 GEMMs + 3 small kernels, stage 1;
     // recording; history: chunk sums, rows; sweep counter
-    int n = 8 + ctx->nphase * ((int)ctx->any_exact + 2 * (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 3;
+    int n = 8 + ctx->ngroup * ctx->nphase * ((int)ctx->any_exact + 2 * (int)ctx->any_fast) + 5 * (int)ctx->any_npt + 3;
     if (ctx->any_npt && (ctx->any_da || ctx->rec_cap > 0)) n += 2;
     if (ctx->any_npt && ctx->any_da) n += 6;
     if (ctx->any_npt && ctx->any_screen) n += 3; // screen energies, chunk sums, stage 1

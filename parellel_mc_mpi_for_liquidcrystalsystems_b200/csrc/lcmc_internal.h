@@ -118,6 +118,8 @@ struct DevView {
     DevStats *stats;    // [R]
     int *act_off;       // [nphase * (R + 1)] active-cell prefix per phase
     int nphase;         // colour phases per sweep: 8, or LCMC_MAX_COLOURS with a fine-grid replica
+    int r_lo, r_hi;     // replicas whose cells the phase kernels attempt (a group of a batch: [r_lo, r_hi))
+    int ngroup;         // replica groups (resc_count/resc_list hold one set of phases per group)
     int *p2r;           // [ntot] replica of each particle slot
     // particle state, cell-sorted (current buffer)
     double *px, *py, *pz, *ox, *oy, *oz;
@@ -138,6 +140,7 @@ struct DevView {
     double *cell_abs;          // per cell: sum of |dE| of the accepted moves
     int *p2c;                  // [ctot] replica of each cell slot
     int *resc_count;           // [nphase] cells the FP32 kernel handed over to the FP64 kernel, per colour phase
+                               // (per group: a group's view points at its own nphase counts and lists)
     int *resc_list;            // [nphase x ctot] their codes: cell * 4 + mode (1 large term, 2 capacity)
     int *cell_fp64;            // per cell: 0 FP32, 1 attempted in FP64 (large term), 2 (capacity)
     unsigned char *outcome;    // [ntot] by particle slot of id: 0/1/2

@@ -76,9 +76,9 @@ __global__ void k_sweep_setup(DevView v)
         p.vol_state = 0;
     }
     __syncthreads();
+    for (int i = threadIdx.x; i < v.nphase * v.ngroup; i += blockDim.x) v.resc_count[i] = 0;
     if ((int)threadIdx.x < v.nphase) {
         int ci = threadIdx.x;
-        v.resc_count[ci] = 0;
         int *off = v.act_off + ci * (v.R + 1);
         int acc = 0;
         for (int r = 0; r < v.R; r++) {

@@ -47,8 +47,8 @@ __global__ void __launch_bounds__(128) k_phase_exact(DevView v, int ci)
     __shared__ int s_cell[4][27];
     __shared__ int s_base[4][28];
     const int *off = v.act_off + ci * (v.R + 1);
-    const int total = off[v.R];
-    for (int a = blockIdx.x * nw + wib; a < total; a += gridDim.x * nw) {
+    const int total = off[v.r_hi]; // this launch's replicas: active cells [off[r_lo], off[r_hi])
+    for (int a = off[v.r_lo] + blockIdx.x * nw + wib; a < total; a += gridDim.x * nw) {
         const int r = find_replica(off, v.R, a);
         const Replica &p = v.rep[r];
         if (p.use_fast) continue;

@@ -284,9 +284,9 @@ __global__ void __launch_bounds__(NT, FastMinBlocks<AMAX>::value) k_phase_fast(c
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const int *off = v.act_off + ci * (v.R + 1);
-    const int total = off[v.R];
+    const int total = off[v.r_hi]; // this launch's replicas: active cells [off[r_lo], off[r_hi])
 
-    for (int a = blockIdx.x; a < total; a += gridDim.x) {
+    for (int a = off[v.r_lo] + blockIdx.x; a < total; a += gridDim.x) {
         const int r = find_replica_f(off, v.R, a);
         const Replica &p = v.rep[r];
         if (!p.use_fast) continue; // uniform across the block

@@ -278,6 +278,37 @@ def test_batched_replicas_match_single_runs():
             assert b.stats(r)["accepted"] == wst["accepted"]
 
 
+def test_replica_groups_match_single_runs():
+    """A batch of nine replicas (FP64 and FP32 kernels, NVT and NPT, with and
+    without a colloid) runs its colour phases as replica groups on their own
+    streams; every replica still reproduces its single run bit for bit."""
+    ps = []
+    for r in range(9):
+        kw = dict(COMMON, num_particles=1000 + 250 * r, system_density=0.30, rng_seed=300 + r,
+                  precision_mode=r % 2, system_temperature=0.9 + 0.05 * r)
+        if r % 3 == 1:
+            kw.update(mc_ensemble_type=2, system_pressure=2.0)
+        if r % 3 == 2:
+            kw.update(colloid_radius=3.0, colloid_wall_option=1)
+        ps.append(lcmc.default_params(**kw))
+    singles = []
+    for p in ps:
+        with lcmc.GBSystem(p) as s:
+            s.get_initial_config()
+            s.sweep(3)
+            singles.append((s.download(), s.stats()))
+    with lcmc.GBSystem(ps) as b:
+        for r in range(len(ps)):
+            b.get_initial_config(r)
+        b.sweep(3)
+        for r, (want, wst) in enumerate(singles):
+            got = b.download(r)
+            for x, y in zip(got[0], want[0]):
+                assert np.array_equal(bits(x), bits(y)), r
+            assert np.array_equal(bits(got[1]), bits(want[1])), r
+            assert b.stats(r)["accepted"] == wst["accepted"] and b.stats(r)["energy"] == wst["energy"], r
+
+
 def test_order_parameter_vs_oracle():
     lp, _ = params_pair(4096, 0.32, 7, init_orientation_cone_deg=20.0)
     state, box = start_state(lp)
