@@ -19,7 +19,10 @@
  * without a CUDA device every device call returns LCMC_ENODEV.
  *
  * Threading: one host thread per context; a context owns one CUDA stream and
- * is not reentrant.
+ * is not reentrant.  A batch of 8 or more replicas also owns one helper
+ * stream per further replica group: inside every sweep the colour phases of
+ * each group run on its stream, forked from the context's stream after the
+ * rebin and joined back into it before the statistics.
  */
 #ifndef LCMC_H
 #define LCMC_H
@@ -228,7 +231,8 @@ int lcmc_record_moves(lcmc_ctx *ctx, int on);
 int lcmc_get_move_records(lcmc_ctx *ctx, int replica, double *dE, double *log_u, int n);
 
 /* ---- measurement (no counterpart in the reference, which only times with clock()) ---- */
-/* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
+/* The CUDA stream (cudaStream_t) of this context: every sweep starts and ends
+ * on it (work enqueued on it after lcmc_sweep returns follows the sweep). */
 int lcmc_get_stream(lcmc_ctx *ctx, void **stream);
 /* Kernel launches in one sweep of this context (all replicas). */
 int lcmc_kernels_per_sweep(lcmc_ctx *ctx);
