@@ -100,3 +100,29 @@ def test_lpt_split_single_rank_and_ties():
     assert bench.lpt_split([3.0, 1.0, 2.0], 1) == [[0, 1, 2]]
     assert bench.lpt_split([5.0, 5.0, 5.0, 5.0], 2) == [[0, 2], [1, 3]]
     assert bench.lpt_split([], 3) == [[], [], []]
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` (the reference's own attempt_monte_carlo_move
+    from oracle/_ref, on the host cores) prints one JSON line with the GPU arm's
+    metric, unit and config, its real timed steps, and e2e equal to value."""
+    import json
+    import subprocess
+
+    import pytest
+    if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "libmcref_omp.so")):
+        pytest.skip("oracle/_ref not built (the reference source was not available at build time)")
+    sys.path.insert(0, REPO)
+    import bench
+    out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--steps", "3",
+                          "--warmup", "1", "--cpu-seconds", "2"], capture_output=True, text=True, timeout=600,
+                         cwd=REPO)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["config"] == bench.WORKLOAD and d["steps"] == 3 and d["warmup"] == 1
+    assert d["value"] > 0 and d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["ms_per_step"] > 0 and d["higher_is_better"] is True
