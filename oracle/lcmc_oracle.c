@@ -528,6 +528,7 @@ static void philox_at(const uint32_t key[2], uint32_t id, uint64_t sweep, uint32
 #define TAG_SHIFT 0x100u
 #define TAG_COLOUR 0x101u    /* and 0x102 */
 #define TAG_VOLUME 0x103u
+#define TAG_COLOUR_EXT 0x110u /* 0x110..0x114: colour order beyond 8 colours (fine grid) */
 #define TAG_INIT 0x200u      /* and 0x201 */
 #define SWEEP_ID 0xFFFFFFFFu /* counter word 0 for per-sweep draws */
 
@@ -671,11 +672,31 @@ int lco_cell_of(double x, double shift, double w, int nc, double L)
     return c;
 }
 
+/* Fine cell grid (cell_grid 1): the largest count of cells at least wmin wide,
+ * odd or even (an odd count >= 3 takes 3 colours on that axis). */
+int lco_grid_dims_fine(double L, double wmin, int fine, int *nc)
+{
+    int m = (int)floor(L / wmin);
+    *nc = m >= 2 ? ((fine && m >= 3) ? m : m - (m & 1)) : 1;
+    return 0;
+}
+
+static int grid_build_nc(lco_grid *g, int n, const double *px, const double *py, const double *pz,
+                         const double box[3], const int nc[3], const double shift[3]);
+
 int lco_grid_build(lco_grid *g, int n, const double *px, const double *py, const double *pz, const double box[3],
                    double wmin, const double shift[3])
 {
+    int nc[3];
+    for (int k = 0; k < 3; k++) lco_grid_dims(box[k], wmin, &nc[k]);
+    return grid_build_nc(g, n, px, py, pz, box, nc, shift);
+}
+
+static int grid_build_nc(lco_grid *g, int n, const double *px, const double *py, const double *pz,
+                         const double box[3], const int nc[3], const double shift[3])
+{
     for (int k = 0; k < 3; k++) {
-        lco_grid_dims(box[k], wmin, &g->nc[k]);
+        g->nc[k] = nc[k];
         g->w[k] = box[k] / (double)g->nc[k];
         g->shift[k] = shift[k];
     }
@@ -852,27 +873,83 @@ static int stage_stencil(const lco_grid *g, int cx, int cy, int cz, int *slots)
     return S;
 }
 
-int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n, double *px, double *py, double *pz,
-              double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st, unsigned char *accept_bits,
-              int *order_out)
+/* Cells of colour b along an axis of nc cells with k colours, and the index of
+ * the j-th of them.  k = 2 (even nc, or a single cell): cells b, b + 2, ...
+ * k = 3 (odd nc >= 3, fine grid), nc = 3q + r: colour i mod 3 for i < 3q, then
+ * r = 1: cell 3q takes colour 1; r = 2: cells 3q, 3q + 1 take colours 0, 1
+ * (neighbours never share a colour, and every colour holds q or q + 1 cells). */
+static int axis_colour_count(int nc, int k, int b)
 {
-    int nc[3];
-    for (int k = 0; k < 3; k++) lco_grid_dims(box[k], c->wmin, &nc[k]);
+    if (k != 3) return (nc - b + 1) / 2;
+    int q = nc / 3, r = nc - 3 * q;
+    return q + ((r >= 1 && b == 1) ? 1 : 0) + ((r == 2 && b == 0) ? 1 : 0);
+}
+static int axis_colour_cell(int nc, int k, int b, int j)
+{
+    if (k != 3) return 2 * j + b;
+    int q = nc / 3, r = nc - 3 * q;
+    return j < q ? b + 3 * j : 3 * q + (r == 2 ? b : 0);
+}
+
+/* Shuffled order of K colours (K = 8: lco_colour_order's draws and result;
+ * more colours draw 4 more words per TAG_COLOUR_EXT call). */
+static void colour_order_k(const uint32_t key[2], uint64_t sweep, int K, int *perm)
+{
+    uint32_t rr[32];
+    uint32_t a[4], b[4];
+    philox_at(key, SWEEP_ID, sweep, TAG_COLOUR, a);
+    philox_at(key, SWEEP_ID, sweep, TAG_COLOUR + 1, b);
+    for (int i = 0; i < 4; i++) {
+        rr[i] = a[i];
+        rr[4 + i] = b[i];
+    }
+    for (int m = 0; 8 + 4 * m < K - 1; m++) {
+        uint32_t e[4];
+        philox_at(key, SWEEP_ID, sweep, TAG_COLOUR_EXT + (uint32_t)m, e);
+        for (int i = 0; i < 4; i++) rr[8 + 4 * m + i] = e[i];
+    }
+    for (int i = 0; i < K; i++) perm[i] = i;
+    for (int i = K - 1; i >= 1; i--) {
+        int j = (int)(rr[K - 1 - i] % (uint32_t)(i + 1));
+        int t = perm[i];
+        perm[i] = perm[j];
+        perm[j] = t;
+    }
+}
+
+/* One checkerboard sweep on the even grid (fine = 0: 8 colours) or on the
+ * fine grid (fine = 1: odd cell counts take 3 colours on their axis, up to 27
+ * colours); see lco_sweep for the move. */
+int lco_sweep_grid(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int fine, int n, double *px,
+                   double *py, double *pz, double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st,
+                   unsigned char *accept_bits, int *order_out)
+{
+    int nc[3], kc[3];
+    for (int k = 0; k < 3; k++) {
+        lco_grid_dims_fine(box[k], c->wmin, fine, &nc[k]);
+        kc[k] = ((nc[k] & 1) && nc[k] >= 3) ? 3 : 2;
+    }
     double shift[3];
     lco_sweep_shift(key, sweep, nc, box, shift);
     lco_grid g;
-    lco_grid_build(&g, n, px, py, pz, box, c->wmin, shift);
-    int perm[8];
-    lco_colour_order(key, sweep, perm);
+    grid_build_nc(&g, n, px, py, pz, box, nc, shift);
+    const int K = kc[0] * kc[1] * kc[2];
+    int perm[27];
+    colour_order_k(key, sweep, K, perm);
     memset(st, 0, sizeof(*st));
     long nb = 0;
     int *slots = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
-    for (int ci = 0; ci < 8; ci++) {
+    for (int ci = 0; ci < K; ci++) {
         int col = perm[ci];
-        int bx = col & 1, by = (col >> 1) & 1, bz = (col >> 2) & 1;
-        for (int cz = bz; cz < g.nc[2]; cz += 2)
-            for (int cy = by; cy < g.nc[1]; cy += 2)
-                for (int cx = bx; cx < g.nc[0]; cx += 2) {
+        int b[3] = {col % kc[0], (col / kc[0]) % kc[1], col / (kc[0] * kc[1])};
+        int cnt[3];
+        for (int a = 0; a < 3; a++) cnt[a] = axis_colour_count(nc[a], kc[a], b[a]);
+        for (int jz = 0; jz < cnt[2]; jz++)
+            for (int jy = 0; jy < cnt[1]; jy++)
+                for (int jx = 0; jx < cnt[0]; jx++) {
+                    const int cx = axis_colour_cell(nc[0], kc[0], b[0], jx);
+                    const int cy = axis_colour_cell(nc[1], kc[1], b[1], jy);
+                    const int cz = axis_colour_cell(nc[2], kc[2], b[2], jz);
                     int cell = (cz * g.nc[1] + cy) * g.nc[0] + cx;
                     const int cc[3] = {cx, cy, cz};
                     int S = stage_stencil(&g, cx, cy, cz, slots);
@@ -895,6 +972,13 @@ int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n,
     free(slots);
     lco_grid_free(&g);
     return 0;
+}
+
+int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n, double *px, double *py, double *pz,
+              double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st, unsigned char *accept_bits,
+              int *order_out)
+{
+    return lco_sweep_grid(c, key, sweep, 0, n, px, py, pz, ox, oy, oz, box, st, accept_bits, order_out);
 }
 
 /* lco_sweep with the active cells of each colour shared among threads

@@ -150,6 +150,13 @@ typedef struct {
 int lco_sweep(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int n, double *px, double *py, double *pz,
               double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st, unsigned char *accept_bits,
               int *order_out);
+/* The same sweep on the even grid (fine = 0, what lco_sweep runs) or on the
+ * fine grid (fine = 1, cell_grid 1: odd cell counts take 3 colours on their
+ * axis, up to 27 colours, drawn and ordered as the GPU's k_sweep_setup does). */
+int lco_sweep_grid(const lco_consts *c, const uint32_t key[2], uint64_t sweep, int fine, int n, double *px,
+                   double *py, double *pz, double *ox, double *oy, double *oz, const double box[3], lco_sweep_stats *st,
+                   unsigned char *accept_bits, int *order_out);
+int lco_grid_dims_fine(double L, double wmin, int fine, int *nc);
 
 /* lco_sweep with each colour's active cells shared among OpenMP threads (in
  * the -fopenmp build, oracle/_build/liblcmc_oracle_omp.so): the same final

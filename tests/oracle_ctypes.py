@@ -95,6 +95,8 @@ def lib():
         L.lco_colour_order.argtypes = [U32P, C.c_uint64, IP]
         L.lco_sweep.argtypes = [C.POINTER(Consts), U32P, C.c_uint64, C.c_int, DP, DP, DP, DP, DP, DP, DP,
                                 C.POINTER(SweepStats), C.POINTER(C.c_ubyte), IP]
+        L.lco_sweep_grid.argtypes = [C.POINTER(Consts), U32P, C.c_uint64, C.c_int, C.c_int, DP, DP, DP, DP, DP, DP, DP,
+                                C.POINTER(SweepStats), C.POINTER(C.c_ubyte), IP]
         L.lco_volume_move.argtypes = [C.POINTER(Consts), U32P, C.c_uint64, D, D, C.c_int, DP, DP, DP, DP, DP, DP,
                                       DP, C.POINTER(VolumeInfo)]
         L.lco_order_parameter.argtypes = [C.c_int, DP, DP, DP, DP, DP, DP]
@@ -154,14 +156,15 @@ def init_lattice(n=1000, rho=0.30, R=0.0, seed=12345, cone=180.0, replica=0, **k
     return (*a, box)
 
 
-def sweep(c, k, sweep_index, state, box, record=False):
-    """One canonical checkerboard sweep on `state` (list of 6 arrays, updated in place)."""
+def sweep(c, k, sweep_index, state, box, record=False, fine=False):
+    """One canonical checkerboard sweep on `state` (list of 6 arrays, updated in
+    place); fine: on the fine cell grid (cell_grid 1)."""
     n = len(state[0])
     st = SweepStats()
     bits = np.zeros(n, dtype=np.uint8) if record else None
     order = np.zeros(n, dtype=np.int32) if record else None
-    lib().lco_sweep(C.byref(c), k, sweep_index, n, *[ptr(x) for x in state], ptr(box), C.byref(st),
-                    ptr(bits, C.c_ubyte) if record else None, ptr(order, C.c_int) if record else None)
+    lib().lco_sweep_grid(C.byref(c), k, sweep_index, int(fine), n, *[ptr(x) for x in state], ptr(box), C.byref(st),
+                         ptr(bits, C.c_ubyte) if record else None, ptr(order, C.c_int) if record else None)
     return st, bits, order
 
 

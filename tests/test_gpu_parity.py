@@ -32,13 +32,13 @@ def bits(a):
     return np.asarray(a, dtype=np.float64).view(np.uint64)
 
 
-def oracle_sweeps(op, state, box, n_sweeps, start=0, npt=False):
+def oracle_sweeps(op, state, box, n_sweeps, start=0, npt=False, fine=False):
     c = oc.consts(op, oc.ARITH_CANONICAL)
     k = oc.key(op.rng_seed)
     outs, vols = [], []
     n = len(state[0])
     for s in range(start, start + n_sweeps):
-        st, b, order = oc.sweep(c, k, s, state, box, record=True)
+        st, b, order = oc.sweep(c, k, s, state, box, record=True, fine=fine)
         o = np.zeros(n, dtype=np.uint8)
         o[order] = b
         outs.append(o)
@@ -110,6 +110,28 @@ def test_fp64_sweeps_bitwise_general_grid():
     want, _ = oracle_sweeps(op, state, box, 2)
     for a, b in zip(got, want):
         assert np.array_equal(a, b)
+    for a, b in zip(g, state):
+        assert np.array_equal(bits(a), bits(b))
+
+
+@pytest.mark.parametrize("n,rho,R", [(4096, 0.32, 0.0), (8000, 0.30, 3.0)])
+def test_fp64_sweeps_bitwise_fine_grid(n, rho, R):
+    """Fine cell grid (cell_grid 1): an odd cell count per axis (5 and 7 here)
+    takes three colours on that axis, 27 colour phases per sweep; the FP64
+    kernel reproduces the oracle's fine-grid sweeps bit for bit (outcomes and
+    coordinates)."""
+    kw = dict(colloid_radius=R, colloid_wall_option=1) if R > 0 else {}
+    lp, op = params_pair(n, rho, 31, precision_mode=0, **kw)
+    lp.cell_grid = 1
+    state, box = start_state(lp)
+    with lcmc.GBSystem(lp) as s:
+        s.set_kernel(0)
+        s.upload(*state, box)
+        got = gpu_sweeps(s, 3)
+        g, _ = s.download()
+    want, _ = oracle_sweeps(op, state, box, 3, fine=True)
+    for i, (a, b) in enumerate(zip(got, want)):
+        assert np.array_equal(a, b), f"sweep {i}: {np.sum(a != b)} outcomes differ"
     for a, b in zip(g, state):
         assert np.array_equal(bits(a), bits(b))
 
