@@ -250,7 +250,7 @@ def test_fine_grid_fp32_decisions_match_fp64():
 
 def test_fp32_npt_ensemble_matches_fp64():
     """The reference never moves the volume, so the FP32 kernel's NPT ensemble
-    is checked against the FP64 kernel's at a configs[1]-style state point
+    is checked against the FP64 kernel's at a colloid NPT state point
     (N = 32,768, P* = 2, T* = 0.9, colloid R = 5, GB(3, 5, 2, 1)): 12
     independent chains per kernel from one compressed start, 300 sweeps of
     burn-in and 2000 recorded; <rho>, <U/N> and <P2> agree within 3.5 standard
