@@ -26,3 +26,37 @@ def test_parallel_sweeps_equal_the_oracle(monkeypatch):
         for u, v in zip(a, b):
             assert np.array_equal(u.view(np.uint64), v.view(np.uint64))
     assert os.environ["OMP_NUM_THREADS"] == "4"
+
+
+def test_fine_grid_sweep_schedule():
+    """The oracle's fine-grid sweep (lco_sweep_grid, fine = 1): with an even cell
+    count it is the even-grid sweep bit for bit (same colours, draws and cell
+    order); with an odd count (5 cells per axis, 27 colours) it attempts every
+    particle exactly once."""
+    import ctypes as C
+    # even: 6 cells per axis at N = 6000, rho* = 0.3 (L = 27.1)
+    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=6000, rho=0.30, seed=72)
+    p = oc.params(num_particles=6000, system_density=0.30, rng_seed=72)
+    c = oc.consts(p, oc.ARITH_CANONICAL)
+    k = oc.key(72)
+    nc = C.c_int()
+    oc.lib().lco_grid_dims_fine.argtypes = [C.c_double, C.c_double, C.c_int, C.POINTER(C.c_int)]
+    oc.lib().lco_grid_dims_fine(box[0], c.wmin, 1, C.byref(nc))
+    assert nc.value % 2 == 0
+    a = [np.ascontiguousarray(x.copy()) for x in (px, py, pz, ox, oy, oz)]
+    b = [np.ascontiguousarray(x.copy()) for x in (px, py, pz, ox, oy, oz)]
+    for s in range(2):
+        _, ba, oa = oc.sweep(c, k, s, a, box, record=True)
+        _, bb, ob = oc.sweep(c, k, s, b, box, record=True, fine=True)
+        assert np.array_equal(oa, ob) and np.array_equal(ba, bb)
+    for u, v in zip(a, b):
+        assert np.array_equal(u.view(np.uint64), v.view(np.uint64))
+    # odd: 5 cells per axis at N = 4096, rho* = 0.32
+    px, py, pz, ox, oy, oz, box = oc.init_lattice(n=4096, rho=0.32, seed=73)
+    p = oc.params(num_particles=4096, system_density=0.32, rng_seed=73)
+    c = oc.consts(p, oc.ARITH_CANONICAL)
+    oc.lib().lco_grid_dims_fine(box[0], c.wmin, 1, C.byref(nc))
+    assert nc.value == 5
+    st = [np.ascontiguousarray(x.copy()) for x in (px, py, pz, ox, oy, oz)]
+    s0, _, order = oc.sweep(c, oc.key(73), 0, st, box, record=True, fine=True)
+    assert s0.attempted == 4096 and sorted(order.tolist()) == list(range(4096))
