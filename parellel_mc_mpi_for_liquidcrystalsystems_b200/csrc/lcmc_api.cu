@@ -88,6 +88,7 @@ struct lcmc_ctx {
     int kernel_override = -1;
     int fast_variant = 0;
     int need_amax = 0; // active-cell capacity the capacity rule asks for
+    int need_min = 0;  // the smallest capacity lcmc_autotune may try: mean + 3 standard deviations of a cell's count
     int tuned_class = -1; // capacity class lcmc_autotune chose (kept while it holds the rule's capacity)
     bool checks_off = false; // no periodic energy checks (autotune trials)
     int grid_elem = 0, grid_exact = 0, grid_fast = 0, grid_energy = 0, grid_screen = 0;
@@ -633,6 +634,18 @@ static int capacity_rule(const lcmc_params &p, double L, double wmin, bool npt)
     return (int)std::ceil(mean + 4.0 * sd + 4.0);
 }
 
+// The smallest capacity the autotuner tries: mean + 3 standard deviations of a
+// cell's count (the caller's cell_capacity when given).  A class between this
+// and the rule's capacity hands a few more cells to the FP64 kernel per sweep,
+// which the timed trials weigh against its higher occupancy.
+static int capacity_floor(const lcmc_params &p, double L, double wmin)
+{
+    if (p.cell_capacity > 0) return p.cell_capacity;
+    double mean, sd;
+    cell_count_stats(p, L, wmin, &mean, &sd);
+    return (int)std::ceil(mean + 3.0 * sd);
+}
+
 // the smallest capacity class that holds `want` (else the largest)
 static int capacity_class(int want)
 {
@@ -687,7 +700,7 @@ static int push_kernel_fields(lcmc_ctx *c)
 static void choose_kernels(lcmc_ctx *c)
 {
     c->any_fast = c->any_exact = c->any_npt = false;
-    int need_amax = 0;
+    int need_amax = 0, need_min = 0;
     bool spec21 = true; // every system has mu = 2, nu = 1, sigma0 = 1
     for (int r = 0; r < c->R; r++) {
         Replica &rp = c->rep[r];
@@ -707,6 +720,7 @@ static void choose_kernels(lcmc_ctx *c)
             if (nc < 6) c->any_exact = true; // NPT boxes near the 4-cell threshold may switch
             const int want = capacity_rule(p, rp.L[0], rp.wmin, rp.ensemble == 2);
             if (want > need_amax) need_amax = want;
+            need_min = std::max(need_min, capacity_floor(p, rp.L[0], rp.wmin));
         } else {
             c->any_exact = true;
         }
@@ -714,8 +728,9 @@ static void choose_kernels(lcmc_ctx *c)
         spec21 = spec21 && p.gb_mu_exponent == 2.0 && p.gb_nu_exponent == 1.0 && p.gb_sigma_sidetoside == 1.0;
     }
     c->need_amax = need_amax;
+    c->need_min = need_min;
     int cls = capacity_class(need_amax);
-    if (c->tuned_class >= 0 && fast_variant(c->tuned_class).amax >= need_amax) cls = c->tuned_class;
+    if (c->tuned_class >= 0 && fast_variant(c->tuned_class).amax >= need_min) cls = c->tuned_class;
     c->fast_variant = 2 * cls + (spec21 ? 1 : 0);
     set_caps(c);
 }
@@ -1752,8 +1767,8 @@ extern "C" int lcmc_autotune(lcmc_ctx *ctx, int sweeps, const char *cache_path, 
             npt4 = npt4 || (ctx->rep[r].ensemble == 2 && grid_dim_host(ctx->rep[r].L[0], ctx->rep[r].wmin, ctx->rep[r].fine) >= 4);
         for (int v = 0; v < fast_variant_count(); v++) {
             if (!ctx->any_fast && v != (ctx->fast_variant >> 1)) continue;
-            // classes below the rule's capacity are not tried (the largest always is)
-            if (ctx->any_fast && fast_variant(v).amax < ctx->need_amax && v != fast_variant_count() - 1) continue;
+            // classes below mean + 3 standard deviations of a cell's count are not tried (the largest always is)
+            if (ctx->any_fast && fast_variant(v).amax < ctx->need_min && v != fast_variant_count() - 1) continue;
             cand.push_back({v, 1});
             if (npt4) cand.push_back({v, 0});
         }
